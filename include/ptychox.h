@@ -1,0 +1,122 @@
+/*
+ * libptychox — C ABI of the B200-native (sm_100a) ptychography operators.
+ *
+ * Conventions shared by every entry point:
+ *   - complex arrays are interleaved complex64 (float re, float im), row-major,
+ *     contiguous, in device memory; they are passed as float* / const float*;
+ *   - positions / LED indices are device int64 pairs (x, y), zero-based;
+ *   - `stream` is a cudaStream_t (NULL = legacy default stream); every launch is
+ *     stream-ordered and nothing synchronises the host;
+ *   - outputs are caller-allocated; temporary frames live in a caller-provided
+ *     workspace whose minimum size the *_workspace_bytes functions return (a larger
+ *     workspace processes more frames per launch);
+ *   - the return value is a status code (PTX_OK = 0); ptx_last_error() gives the
+ *     calling thread's last message.
+ *
+ * Gradients follow PyTorch's convention for complex inputs of a real loss
+ * (dL/dRe + i dL/dIm), as the reference's hand-written backward functions do.
+ *
+ * Reference interfaces replaced (THUHoloLab/PtychoX, python/ptychoX/csrc):
+ *   pybind11 `_C.forward` / `_C.backward` / `_C.clear_plan_cache` of
+ *   base_extension.cpp:21-66, fpm_extension.cpp:21-66, coded_extension.cpp:26-94.
+ */
+#ifndef PTYCHOX_H_
+#define PTYCHOX_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------- */
+#define PTX_OK 0
+#define PTX_ERR_INVALID_ARGUMENT 1  /* bad pointer, shape or scalar          -> ValueError   */
+#define PTX_ERR_UNSUPPORTED_SIZE 2  /* frame side not {2,3,5}-smooth / too big -> ValueError   */
+#define PTX_ERR_WORKSPACE 3         /* workspace smaller than one frame      -> RuntimeError */
+#define PTX_ERR_CUDA 4              /* CUDA launch / runtime error           -> RuntimeError */
+#define PTX_ERR_OUT_OF_BOUNDS 5     /* a scan window leaves the object       -> ValueError   */
+#define PTX_ERR_TIMEOUT 6           /* a bounded device wait gave up         -> RuntimeError */
+
+/* ---- library ------------------------------------------------------------------- */
+
+/* Library version as 10000*major + 100*minor + patch. */
+int ptx_version(void);
+
+/* Message of the calling thread's last failed call ("" if none). */
+const char* ptx_last_error(void);
+
+/* Drop cached FFT plans (twiddle tables are rebuilt on next use).
+ * Replaces `_C.clear_plan_cache` (base_extension.cpp:65, fpm_extension.cpp:65,
+ * coded_extension.cpp:93) and ptychoX.clear_cuda_plan_cache (ptychoX/__init__.py:10-13). */
+int ptx_clear_cache(void);
+
+/* Number of kernels this library has launched in the process (all devices). */
+long long ptx_launch_count(void);
+
+/* Optional per-kernel CUDA-event timing: when enabled every launch is bracketed by an
+ * event pair on its stream.  ptx_profile_read synchronises on the recorded events and
+ * returns the accumulated device time and timed launches of one kernel kind
+ * (ids 0 .. ptx_profile_kinds()-1, named by ptx_profile_name). */
+int ptx_profile_enable(int on);
+int ptx_profile_reset(void);
+int ptx_profile_kinds(void);
+int ptx_profile_read(int kernel_id, double* total_ms, long long* launches);
+const char* ptx_profile_name(int kernel_id);
+
+/* 1 if `n` is a supported transform length (n = 2^a 3^b 5^c, 2 <= n <= 1024). */
+int ptx_fft_supported(int n);
+
+/* Build the twiddle table for length n on the current device now (it is otherwise
+ * built on first use, which must not happen inside a CUDA graph capture). */
+int ptx_fft_prepare(int n);
+
+/* ---- conventional ptychography --------------------------------------------------
+ * Operator  A[b] = |fftshift(fft2(sample[y_b:y_b+ph, x_b:x_b+pw] * probe))|.
+ * Replaces `_C.forward` / `_C.backward` of base_extension.cpp:21-60 and the torch path
+ * of python/ptychoX/base/ops.py:41-107.
+ */
+
+/* Minimum workspace for the base entry points (frames processed per launch = as many
+ * as fit; `batch` caps what is useful). */
+size_t ptx_base_workspace_bytes(int probe_h, int probe_w, int batch);
+
+/* Forward.  far_field: complex64 [batch, ph, pw], the fftshifted far field (may be
+ * NULL when not needed); amplitude: float32 [batch, ph, pw].
+ * Replaces base_extension.cpp:21-32 (ptychox_base_forward_cuda, base_kernel.cu:302-329). */
+int ptx_base_forward(const float* sample, int sample_h, int sample_w,
+                     const float* probe, int probe_h, int probe_w,
+                     const int64_t* positions_xy, int batch,
+                     float* far_field, float* amplitude,
+                     void* workspace, size_t workspace_bytes, void* stream);
+
+/* Adjoint of the forward for an upstream gradient grad_output (float32 [batch, ph, pw]):
+ * grad_sample (complex64 [H, W]) and grad_probe (complex64 [ph, pw]) are OVERWRITTEN.
+ * far_field is the array written by ptx_base_forward; the object patches are re-read
+ * from `sample` instead of being saved.
+ * Replaces base_extension.cpp:34-60 (ptychox_base_backward_cuda, base_kernel.cu:331-357). */
+int ptx_base_backward(const float* grad_output, const float* far_field,
+                      const float* sample, int sample_h, int sample_w,
+                      const float* probe, int probe_h, int probe_w,
+                      const int64_t* positions_xy, int batch,
+                      float* grad_sample, float* grad_probe,
+                      void* workspace, size_t workspace_bytes, void* stream);
+
+/* Fused sweep: forward, amplitude-MSE loss against uint16 counts, adjoint.
+ * loss (device double[1]) = mean((A - sqrt(scale * I))^2) accumulated in FP64;
+ * grad_sample / grad_probe are OVERWRITTEN with dloss/d(sample, probe).
+ * Equivalent to F.mse_loss(ptychoX_base(...), observed).backward()
+ * (python/train_ptychography.py:549-557) with observed = sqrt(float32(I) * scale). */
+int ptx_base_sweep(const float* sample, int sample_h, int sample_w,
+                   const float* probe, int probe_h, int probe_w,
+                   const int64_t* positions_xy, int batch,
+                   const uint16_t* measured, float scale,
+                   double* loss, float* grad_sample, float* grad_probe,
+                   void* workspace, size_t workspace_bytes, void* stream);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#endif /* PTYCHOX_H_ */

@@ -1,0 +1,25 @@
+"""ptychox_b200 — B200-native (sm_100a) PtychoX operators behind the reference's API.
+
+Drop-in for ``python/ptychoX`` (``__init__.py:1-27`` of THUHoloLab/PtychoX): the same
+operator names, aliases and cache hooks, backed by ``libptychox`` (C ABI in
+``include/ptychox.h``).  Added: fused forward+loss+adjoint sweeps (``*_loss``).
+"""
+
+from ._utils import matlab_positions_to_torch
+from .base import clear_cuda_plan_cache as clear_base_cuda_plan_cache
+from .base import ptychoX_base, ptychoX_base_loss, ptychography_base
+
+
+def clear_cuda_plan_cache() -> None:
+    """Drop cached FFT plans of every modality (one shared library cache)."""
+    clear_base_cuda_plan_cache()
+
+
+__all__ = [
+    "clear_cuda_plan_cache",
+    "clear_base_cuda_plan_cache",
+    "ptychoX_base",
+    "ptychoX_base_loss",
+    "ptychography_base",
+    "matlab_positions_to_torch",
+]

@@ -1,0 +1,158 @@
+"""Conventional ptychography operator on the sm_100a library.
+
+Drop-in for ``python/ptychoX/base/ops.py``: ``ptychoX_base`` / ``ptychography_base`` keep
+the reference signature (:14-28) and the ``autograd.Function`` contract (forward saves
+what backward needs, backward returns one gradient per input, :41-107).  Differences by
+design: the only implementation is the CUDA library (``use_cuda_kernels`` is accepted
+and ignored), and windows leaving the sample raise ``ValueError``.
+
+``ptychoX_base_loss`` is the fused sweep: forward, amplitude-MSE against uint16 counts
+and adjoint in one library call, returned as a differentiable FP64 scalar.
+"""
+
+from __future__ import annotations
+
+import torch
+
+from . import _abi
+from ._utils import (
+    as_u16,
+    check_complex_scan_inputs,
+    device_positions,
+    ptr,
+    require_cuda_complex64,
+    stream_handle,
+    workspace,
+)
+
+__all__ = [
+    "ptychoX_base",
+    "ptychography_base",
+    "ptychoX_base_loss",
+    "clear_cuda_plan_cache",
+    "PtychoXBaseFunction",
+    "PtychoXBaseLossFunction",
+]
+
+
+def ptychoX_base(
+    sample: torch.Tensor,
+    probe: torch.Tensor,
+    positions_xy: torch.Tensor,
+    use_cuda_kernels: bool = False,
+) -> torch.Tensor:
+    """Return ``abs(fftshift(fft2(crop(sample) * probe)))``.
+
+    Args:
+        sample: complex object tensor, shape ``[sample_h, sample_w]``.
+        probe: complex probe tensor, shape ``[probe_h, probe_w]``.
+        positions_xy: zero-based ``(x, y)`` scan positions, shape ``[batch, 2]``.
+        use_cuda_kernels: accepted for compatibility; the sm_100a path always runs.
+    """
+    return PtychoXBaseFunction.apply(sample, probe, positions_xy, use_cuda_kernels)
+
+
+ptychography_base = ptychoX_base
+
+
+def clear_cuda_plan_cache() -> None:
+    _abi.call("ptx_clear_cache")
+
+
+def _prepare(sample, probe, positions_xy):
+    check_complex_scan_inputs(sample, probe, positions_xy)
+    require_cuda_complex64(("sample", sample), ("probe", probe))
+    sample = sample.contiguous()
+    probe = probe.contiguous()
+    pos = device_positions(positions_xy, sample.device, tuple(probe.shape), tuple(sample.shape))
+    return sample, probe, pos
+
+
+class PtychoXBaseFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, sample, probe, positions_xy, use_cuda_kernels=False):  # type: ignore[override]
+        sample, probe, pos = _prepare(sample, probe, positions_xy)
+        dev = sample.device
+        batch = pos.shape[0]
+        ph, pw = probe.shape
+        far = torch.empty((batch, ph, pw), dtype=torch.complex64, device=dev)
+        amp = torch.empty((batch, ph, pw), dtype=torch.float32, device=dev)
+        ws_bytes = _abi.query("ptx_base_workspace_bytes", ph, pw, batch)
+        ws = workspace(ws_bytes, dev)
+        with torch.cuda.device(dev):
+            _abi.call("ptx_base_forward", ptr(sample), sample.shape[0], sample.shape[1], ptr(probe), ph, pw,
+                      ptr(pos), batch, ptr(far), ptr(amp), ptr(ws), ws_bytes, stream_handle(dev))
+        ctx.save_for_backward(sample, probe, far, pos)
+        return amp
+
+    @staticmethod
+    def backward(ctx, grad_output):  # type: ignore[override]
+        sample, probe, far, pos = ctx.saved_tensors
+        dev = sample.device
+        batch = pos.shape[0]
+        ph, pw = probe.shape
+        grad_output = grad_output.to(dtype=torch.float32).contiguous()
+        grad_sample = torch.empty_like(sample)
+        grad_probe = torch.empty_like(probe)
+        ws_bytes = _abi.query("ptx_base_workspace_bytes", ph, pw, batch)
+        ws = workspace(ws_bytes, dev)
+        with torch.cuda.device(dev):
+            _abi.call("ptx_base_backward", ptr(grad_output), ptr(far), ptr(sample), sample.shape[0],
+                      sample.shape[1], ptr(probe), ph, pw, ptr(pos), batch, ptr(grad_sample), ptr(grad_probe),
+                      ptr(ws), ws_bytes, stream_handle(dev))
+        return grad_sample, grad_probe, None, None
+
+
+def base_sweep(sample, probe, positions, measured, scale, ws=None):
+    """Run one fused sweep on validated device tensors; returns ``(loss, grad_sample, grad_probe)``.
+
+    ``positions`` must already be int64 on the device and inside the sample; ``measured``
+    uint16 ``[batch, ph, pw]`` in the fftshifted layout of the forward output.
+    """
+    dev = sample.device
+    batch = positions.shape[0]
+    ph, pw = probe.shape
+    loss = torch.empty((), dtype=torch.float64, device=dev)
+    gs = torch.empty_like(sample)
+    gp = torch.empty_like(probe)
+    if ws is None:
+        ws = workspace(_abi.query("ptx_base_workspace_bytes", ph, pw, batch), dev)
+    with torch.cuda.device(dev):
+        _abi.call("ptx_base_sweep", ptr(sample), sample.shape[0], sample.shape[1], ptr(probe), ph, pw,
+                  ptr(positions), batch, ptr(measured), float(scale), ptr(loss), ptr(gs), ptr(gp), ptr(ws),
+                  ws.numel(), stream_handle(dev))
+    return loss, gs, gp
+
+
+class PtychoXBaseLossFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, sample, probe, positions_xy, measured, scale):  # type: ignore[override]
+        sample, probe, pos = _prepare(sample, probe, positions_xy)
+        meas = as_u16(measured, sample.device)
+        if tuple(meas.shape) != (pos.shape[0], probe.shape[0], probe.shape[1]):
+            raise ValueError("measured must have shape [batch, probe_h, probe_w].")
+        loss, gs, gp = base_sweep(sample, probe, pos, meas, scale)
+        ctx.save_for_backward(gs, gp)
+        return loss
+
+    @staticmethod
+    def backward(ctx, grad_loss):  # type: ignore[override]
+        gs, gp = ctx.saved_tensors
+        g = grad_loss.to(torch.float32)
+        return gs * g, gp * g, None, None, None
+
+
+def ptychoX_base_loss(
+    sample: torch.Tensor,
+    probe: torch.Tensor,
+    positions_xy: torch.Tensor,
+    measured: torch.Tensor,
+    scale: float,
+) -> torch.Tensor:
+    """Fused ``F.mse_loss(ptychoX_base(sample, probe, positions), sqrt(scale * measured))``.
+
+    ``measured`` holds uint16 photon counts ``[batch, ph, pw]`` in the fftshifted layout
+    of ``ptychoX_base``'s output.  Returns an FP64 scalar; ``.backward()`` gives
+    ``sample.grad`` / ``probe.grad`` exactly as the unfused composition does.
+    """
+    return PtychoXBaseLossFunction.apply(sample, probe, positions_xy, measured, scale)

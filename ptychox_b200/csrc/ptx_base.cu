@@ -1,0 +1,448 @@
+// Conventional ptychography: forward, adjoint and the fused forward+loss+adjoint sweep.
+//
+// Math (python/ptychoX/base/ops.py:59-67 forward, :92-105 adjoint):
+//   F_b = fft2(O[y_b:y_b+ph, x_b:x_b+pw] * P),   A_b = |fftshift(F_b)|
+//   G_b = ifft2(ifftshift(g_b * F/max(|F|, eps))) * ph*pw
+//   grad_O[window_b] += G_b conj(P),   grad_P += sum_b G_b conj(O_window_b)
+//
+// The 2-D transforms are split into a row pass and a column pass, and every pointwise
+// step is fused into the pass that holds the data:
+//   row pass   (gather O rows x probe rows, row DFT)                      -> scratch
+//   col pass   (column DFT, |F|, residual vs sqrt(scale I), loss, phase,
+//               inverse column DFT)                                        -> scratch
+//   row pass   (inverse row DFT, scatter G conj(P) into grad_O with float2
+//               atomics, accumulate G conj(O) for grad_P in registers)
+// so exit waves and far fields never exist as separate arrays.  Scratch frames use a
+// tiled layout [frame][tile][row][16] so both passes move contiguous runs.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "ptx_internal.h"
+
+namespace ptx {
+namespace {
+
+constexpr size_t kHeaderBytes = 256;           // error word + padding
+constexpr size_t kTargetScratch = 64u << 20;   // frames per launch sized to ~L2
+constexpr float kEps = 1.1920928955078125e-07f;  // torch.finfo(float32).eps
+
+enum ColMode { kColSweep = 0, kColForward = 1, kColBackward = 2 };
+
+__device__ __forceinline__ bool window_ok(long long x0, long long y0, int ph, int pw, int H, int W) {
+  return x0 >= 0 && y0 >= 0 && x0 + pw <= W && y0 + ph <= H;
+}
+
+// Row pass 1: gather O rows, multiply by the probe, forward row DFT, store tiled.
+template <int NR>
+__global__ void __launch_bounds__(256) base_rows_forward(
+    const float2* __restrict__ sample, int H, int W, const float2* __restrict__ probe, int ph, int pw,
+    const int64_t* __restrict__ pos, int nframes, int frames_per_cta, float2* __restrict__ scratch,
+    LinePlan plan, int lines, unsigned* __restrict__ err) {
+  extern __shared__ float2 sm[];
+  const int pitch = line_pitch(pw);
+  const int tid = threadIdx.x;
+  const int l = tid / plan.threads;
+  const int t = (l < lines) ? tid - l * plan.threads : plan.threads;
+  const int r0 = blockIdx.x * lines;
+  const int nrows = min(lines, ph - r0);
+  const int tiles = num_tiles(pw);
+  const int f0 = blockIdx.y * frames_per_cta;
+  const int f1 = min(nframes, f0 + frames_per_cta);
+  float2* my_line = sm + min(l, lines - 1) * pitch;
+  for (int f = f0; f < f1; ++f) {
+    const long long x0 = pos[2 * f], y0 = pos[2 * f + 1];
+    const bool ok = window_ok(x0, y0, ph, pw, H, W);
+    if (!ok && tid == 0) atomicOr(err, 1u);
+    for (int i = tid; i < nrows * pw; i += blockDim.x) {
+      const int li = i / pw, c = i - li * pw;
+      const int r = r0 + li;
+      float2 v = make_float2(0.f, 0.f);
+      if (ok) v = cmul(sample[(y0 + r) * W + x0 + c], __ldg(&probe[r * pw + c]));
+      sm[li * pitch + c] = v;
+    }
+    __syncthreads();
+    line_fft<NR, false>(my_line, plan, t);
+    const int run = nrows * kTile;
+    for (int i = tid; i < tiles * run; i += blockDim.x) {
+      const int ct = i / run;
+      const int rem = i - ct * run;
+      const int li = rem / kTile, cc = rem - li * kTile;
+      const int c = ct * kTile + cc;
+      if (c < pw) scratch[(((size_t)f * tiles + ct) * ph + r0 + li) * kTile + cc] = sm[li * pitch + c];
+    }
+    __syncthreads();
+  }
+}
+
+// Column pass.  kColSweep: column DFT, loss epilogue, inverse column DFT (in place).
+// kColForward: column DFT, write fftshifted far field and amplitude.
+// kColBackward: build g F/|F| from the saved far field, inverse column DFT.
+template <int MODE, int NC>
+__global__ void __launch_bounds__(512, 1) base_cols(
+    float2* __restrict__ scratch, int ph, int pw, int frame0, LinePlan plan, int cols,
+    const uint16_t* __restrict__ measured, float scale, float grad_scale, double inv_numel,
+    double* __restrict__ loss, float2* __restrict__ far_field, float* __restrict__ amplitude,
+    const float* __restrict__ grad_output) {
+  extern __shared__ float2 sm[];
+  __shared__ double red[32];
+  const int pitch = line_pitch(ph);
+  const int tid = threadIdx.x;
+  const int l = tid / plan.threads;
+  const int t = (l < cols) ? tid - l * plan.threads : plan.threads;
+  const int subs = kTile / cols;
+  const int ct = blockIdx.x / subs;
+  const int c0 = ct * kTile + (blockIdx.x - ct * subs) * cols;  // first column of this CTA
+  const int f = blockIdx.y;
+  const int tiles = num_tiles(pw);
+  const int ncols = max(0, min(cols, pw - c0));
+  float2* frame = scratch + ((size_t)f * tiles + ct) * ph * kTile + (c0 - ct * kTile);
+  const size_t g = (size_t)frame0 + f;
+  float2* my_line = sm + min(l, cols - 1) * pitch;
+  const int hh = ph / 2, hw = pw / 2;
+  const int nel = ph * cols;
+
+  if (MODE != kColBackward) {
+    for (int i = tid; i < nel; i += blockDim.x) {
+      const int n = i / cols, cc = i - n * cols;
+      sm[cc * pitch + n] = (cc < ncols) ? frame[n * kTile + cc] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    line_fft<NC, false>(my_line, plan, t);
+  }
+
+  if (MODE == kColSweep) {
+    double acc = 0.0;
+    for (int i = tid; i < nel; i += blockDim.x) {
+      const int n = i / cols, cc = i - n * cols;
+      if (cc >= ncols) continue;
+      const int kc = c0 + cc;
+      int ir = n + hh; if (ir >= ph) ir -= ph;
+      int ic = kc + hw; if (ic >= pw) ic -= pw;
+      const size_t idx = (g * ph + ir) * pw + ic;
+      const float y = sqrtf(static_cast<float>(measured[idx]) * scale);
+      const float2 F = sm[cc * pitch + n];
+      const float a = cabsf(F);
+      const float r = a - y;
+      acc += static_cast<double>(r) * static_cast<double>(r);
+      sm[cc * pitch + n] = cscale(F, grad_scale * r / fmaxf(a, kEps));
+    }
+    // block reduction of the FP64 loss partial
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((tid & 31) == 0) red[tid >> 5] = acc;
+    __syncthreads();
+    if (tid < 32) {
+      const int nw = (blockDim.x + 31) >> 5;
+      double v = (tid < nw) ? red[tid] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (tid == 0) atomicAdd(loss, v * inv_numel);
+    }
+  } else if (MODE == kColForward) {
+    for (int i = tid; i < nel; i += blockDim.x) {
+      const int n = i / cols, cc = i - n * cols;
+      if (cc >= ncols) continue;
+      const int kc = c0 + cc;
+      int ir = n + hh; if (ir >= ph) ir -= ph;
+      int ic = kc + hw; if (ic >= pw) ic -= pw;
+      const size_t idx = (g * ph + ir) * pw + ic;
+      const float2 F = sm[cc * pitch + n];
+      if (far_field) far_field[idx] = F;
+      amplitude[idx] = cabsf(F);
+    }
+    return;
+  } else {  // kColBackward
+    for (int i = tid; i < nel; i += blockDim.x) {
+      const int n = i / cols, cc = i - n * cols;
+      float2 v = make_float2(0.f, 0.f);
+      if (cc < ncols) {
+        const int kc = c0 + cc;
+        int ir = n + hh; if (ir >= ph) ir -= ph;
+        int ic = kc + hw; if (ic >= pw) ic -= pw;
+        const size_t idx = (g * ph + ir) * pw + ic;
+        const float2 F = far_field[idx];
+        v = cscale(F, grad_output[idx] / fmaxf(cabsf(F), kEps));
+      }
+      sm[cc * pitch + n] = v;
+    }
+  }
+  __syncthreads();
+  line_fft<NC, true>(my_line, plan, t);
+  for (int i = tid; i < nel; i += blockDim.x) {
+    const int n = i / cols, cc = i - n * cols;
+    if (cc < ncols) frame[n * kTile + cc] = sm[cc * pitch + n];
+  }
+}
+
+// Row pass 2: inverse row DFT, scatter G conj(P) into grad_O, accumulate G conj(O).
+constexpr int kOwn = kValuesPerThread;  // elements of a line owned by one thread
+
+template <int NR>
+__global__ void __launch_bounds__(256) base_rows_adjoint(
+    const float2* __restrict__ scratch, const float2* __restrict__ sample, int H, int W,
+    const float2* __restrict__ probe, int ph, int pw, const int64_t* __restrict__ pos, int nframes,
+    int frames_per_cta, float2* __restrict__ grad_sample, float2* __restrict__ grad_probe,
+    LinePlan plan, int lines) {
+  extern __shared__ float2 sm[];
+  const int pitch = line_pitch(pw);
+  const int tid = threadIdx.x;
+  const int l = tid / plan.threads;
+  const bool own = l < lines;
+  const int t = own ? tid - l * plan.threads : plan.threads;
+  const int r0 = blockIdx.x * lines;
+  const int nrows = min(lines, ph - r0);
+  const int r = r0 + l;
+  const bool row_ok = own && r < ph;
+  const int tiles = num_tiles(pw);
+  const int f0 = blockIdx.y * frames_per_cta;
+  const int f1 = min(nframes, f0 + frames_per_cta);
+  float2* my_line = sm + min(l, lines - 1) * pitch;
+
+  float2 pconj[kOwn];
+  float2 acc[kOwn];
+#pragma unroll
+  for (int k = 0; k < kOwn; ++k) {
+    const int c = t + k * plan.threads;
+    acc[k] = make_float2(0.f, 0.f);
+    pconj[k] = (row_ok && c < pw) ? cconj(__ldg(&probe[r * pw + c])) : make_float2(0.f, 0.f);
+  }
+  for (int f = f0; f < f1; ++f) {
+    const long long x0 = pos[2 * f], y0 = pos[2 * f + 1];
+    const bool ok = window_ok(x0, y0, ph, pw, H, W);
+    const int run = nrows * kTile;
+    for (int i = tid; i < tiles * run; i += blockDim.x) {
+      const int ct = i / run;
+      const int rem = i - ct * run;
+      const int li = rem / kTile, cc = rem - li * kTile;
+      const int c = ct * kTile + cc;
+      if (c < pw) sm[li * pitch + c] = scratch[(((size_t)f * tiles + ct) * ph + r0 + li) * kTile + cc];
+    }
+    __syncthreads();
+    line_fft<NR, true>(my_line, plan, t);
+    if (row_ok && ok) {
+      const float2* orow = sample + (y0 + r) * W + x0;
+      float2* grow = grad_sample + (y0 + r) * W + x0;
+#pragma unroll
+      for (int k = 0; k < kOwn; ++k) {
+        const int c = t + k * plan.threads;
+        if (c < pw) {
+          const float2 G = my_line[c];
+          atomicAdd(&grow[c], cmul(G, pconj[k]));
+          acc[k] = cadd(acc[k], cmulc(G, orow[c]));
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (row_ok) {
+#pragma unroll
+    for (int k = 0; k < kOwn; ++k) {
+      const int c = t + k * plan.threads;
+      if (c < pw) atomicAdd(&grad_probe[r * pw + c], acc[k]);
+    }
+  }
+}
+
+struct BaseGeom {
+  int H, W, ph, pw, batch;
+  LinePlan row, col;
+  RowShape rs;
+  ColShape cs;
+  size_t frame_bytes;
+  int chunk;
+  unsigned* err;
+  float2* scratch;
+};
+
+int check_common(const void* sample, int H, int W, const void* probe, int ph, int pw,
+                 const int64_t* pos, int batch, void* ws, size_t ws_bytes, BaseGeom* g) {
+  if (!sample || !probe || (!pos && batch > 0) || !ws) {
+    return set_error(PTX_ERR_INVALID_ARGUMENT, "null pointer argument");
+  }
+  if (H <= 0 || W <= 0 || ph <= 0 || pw <= 0 || batch < 0) {
+    return set_error(PTX_ERR_INVALID_ARGUMENT, "non-positive shape");
+  }
+  if (ph > H || pw > W) {
+    return set_error(PTX_ERR_INVALID_ARGUMENT, "probe (%d x %d) larger than sample (%d x %d)", ph, pw, H, W);
+  }
+  g->H = H; g->W = W; g->ph = ph; g->pw = pw; g->batch = batch;
+  if (int st = get_line_plan(pw, &g->row)) return st;
+  if (int st = get_line_plan(ph, &g->col)) return st;
+  g->rs = row_shape(g->row, ph);
+  g->cs = col_shape(g->col);
+  g->frame_bytes = (size_t)num_tiles(pw) * kTile * ph * sizeof(float2);
+  if (ws_bytes < kHeaderBytes + g->frame_bytes) {
+    return set_error(PTX_ERR_WORKSPACE, "workspace of %zu bytes is smaller than one frame (%zu)",
+                     ws_bytes, kHeaderBytes + g->frame_bytes);
+  }
+  const size_t fit = (ws_bytes - kHeaderBytes) / g->frame_bytes;
+  g->chunk = static_cast<int>(std::min<size_t>(fit, (size_t)std::max(batch, 1)));
+  g->err = reinterpret_cast<unsigned*>(ws);
+  g->scratch = reinterpret_cast<float2*>(static_cast<char*>(ws) + kHeaderBytes);
+  int st = PTX_OK;
+  dispatch_len(pw, [&](auto NT) {
+    constexpr int N = decltype(NT)::value;
+    if (!st) st = ensure_smem((const void*)base_rows_forward<N>, g->rs.smem);
+    if (!st) st = ensure_smem((const void*)base_rows_adjoint<N>, g->rs.smem);
+  });
+  dispatch_len(ph, [&](auto NT) {
+    constexpr int N = decltype(NT)::value;
+    if (!st) st = ensure_smem((const void*)base_cols<kColSweep, N>, g->cs.smem);
+    if (!st) st = ensure_smem((const void*)base_cols<kColForward, N>, g->cs.smem);
+    if (!st) st = ensure_smem((const void*)base_cols<kColBackward, N>, g->cs.smem);
+  });
+  if (st) return st;
+  return PTX_OK;
+}
+
+int frames_per_cta_for(int rowgroups, int nframes, int target_ctas) {
+  const long long ctas_one = (long long)rowgroups * nframes;
+  int fpc = static_cast<int>(ctas_one / std::max(target_ctas, 1));
+  return std::max(1, std::min(fpc, nframes));
+}
+
+void launch_rows_forward(const BaseGeom& g, const float2* sample, const float2* probe, const int64_t* pos,
+                         int nframes, cudaStream_t s) {
+  const int rowgroups = (g.ph + g.rs.lines - 1) / g.rs.lines;
+  dim3 grid(rowgroups, nframes);
+  prof_begin(kBaseRowsForward, s);
+  dispatch_len(g.pw, [&](auto NT) {
+    constexpr int N = decltype(NT)::value;
+    base_rows_forward<N><<<grid, g.rs.threads, g.rs.smem, s>>>(sample, g.H, g.W, probe, g.ph, g.pw, pos,
+                                                               nframes, 1, g.scratch, g.row, g.rs.lines, g.err);
+  });
+  prof_end(kBaseRowsForward, s);
+}
+
+void launch_rows_adjoint(const BaseGeom& g, const float2* sample, const float2* probe, const int64_t* pos,
+                         int nframes, float2* grad_sample, float2* grad_probe, cudaStream_t s) {
+  const int rowgroups = (g.ph + g.rs.lines - 1) / g.rs.lines;
+  const int fpc = frames_per_cta_for(rowgroups, nframes, sm_count() * 8);
+  dim3 grid(rowgroups, (nframes + fpc - 1) / fpc);
+  prof_begin(kBaseRowsAdjoint, s);
+  dispatch_len(g.pw, [&](auto NT) {
+    constexpr int N = decltype(NT)::value;
+    base_rows_adjoint<N><<<grid, g.rs.threads, g.rs.smem, s>>>(g.scratch, sample, g.H, g.W, probe, g.ph, g.pw,
+                                                               pos, nframes, fpc, grad_sample, grad_probe, g.row,
+                                                               g.rs.lines);
+  });
+  prof_end(kBaseRowsAdjoint, s);
+}
+
+template <int MODE>
+void launch_cols(const BaseGeom& g, int frame0, int nframes, const uint16_t* measured, float scale,
+                 float grad_scale, double inv_numel, double* loss, float2* far_field, float* amplitude,
+                 const float* grad_output, cudaStream_t s) {
+  dim3 grid(num_tiles(g.pw) * (kTile / g.cs.cols), nframes);
+  prof_begin(kBaseCols, s);
+  dispatch_len(g.ph, [&](auto NT) {
+    constexpr int N = decltype(NT)::value;
+    base_cols<MODE, N><<<grid, g.cs.threads, g.cs.smem, s>>>(g.scratch, g.ph, g.pw, frame0, g.col, g.cs.cols,
+                                                             measured, scale, grad_scale, inv_numel, loss,
+                                                             far_field, amplitude, grad_output);
+  });
+  prof_end(kBaseCols, s);
+}
+
+}  // namespace
+}  // namespace ptx
+
+using namespace ptx;
+
+extern "C" {
+
+size_t ptx_base_workspace_bytes(int probe_h, int probe_w, int batch) {
+  if (probe_h <= 0 || probe_w <= 0) return 0;
+  const size_t frame = (size_t)num_tiles(probe_w) * kTile * probe_h * sizeof(float2);
+  size_t frames = std::max<size_t>(1, kTargetScratch / frame);
+  frames = std::min<size_t>(frames, (size_t)std::max(batch, 1));
+  return kHeaderBytes + frames * frame;
+}
+
+int ptx_base_forward(const float* sample, int sample_h, int sample_w, const float* probe, int probe_h,
+                     int probe_w, const int64_t* positions_xy, int batch, float* far_field, float* amplitude,
+                     void* workspace, size_t workspace_bytes, void* stream) {
+  BaseGeom g;
+  if (int st = check_common(sample, sample_h, sample_w, probe, probe_h, probe_w, positions_xy, batch, workspace,
+                            workspace_bytes, &g)) {
+    return st;
+  }
+  if (!amplitude) return set_error(PTX_ERR_INVALID_ARGUMENT, "amplitude is null");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaMemsetAsync(g.err, 0, sizeof(unsigned), s);
+  const float2* S = reinterpret_cast<const float2*>(sample);
+  const float2* P = reinterpret_cast<const float2*>(probe);
+  for (int b0 = 0; b0 < batch; b0 += g.chunk) {
+    const int nf = std::min(g.chunk, batch - b0);
+    launch_rows_forward(g, S, P, positions_xy + 2 * (size_t)b0, nf, s);
+    launch_cols<kColForward>(g, b0, nf, nullptr, 0.f, 0.f, 0.0, nullptr, reinterpret_cast<float2*>(far_field),
+                             amplitude, nullptr, s);
+  }
+  return cuda_status(cudaGetLastError(), "ptx_base_forward launch");
+}
+
+int ptx_base_backward(const float* grad_output, const float* far_field, const float* sample, int sample_h,
+                      int sample_w, const float* probe, int probe_h, int probe_w, const int64_t* positions_xy,
+                      int batch, float* grad_sample, float* grad_probe, void* workspace, size_t workspace_bytes,
+                      void* stream) {
+  BaseGeom g;
+  if (int st = check_common(sample, sample_h, sample_w, probe, probe_h, probe_w, positions_xy, batch, workspace,
+                            workspace_bytes, &g)) {
+    return st;
+  }
+  if (!grad_output || !far_field || !grad_sample || !grad_probe) {
+    return set_error(PTX_ERR_INVALID_ARGUMENT, "null pointer argument");
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  float2* GS = reinterpret_cast<float2*>(grad_sample);
+  float2* GP = reinterpret_cast<float2*>(grad_probe);
+  cudaMemsetAsync(GS, 0, sizeof(float2) * (size_t)sample_h * sample_w, s);
+  cudaMemsetAsync(GP, 0, sizeof(float2) * (size_t)probe_h * probe_w, s);
+  const float2* S = reinterpret_cast<const float2*>(sample);
+  const float2* P = reinterpret_cast<const float2*>(probe);
+  for (int b0 = 0; b0 < batch; b0 += g.chunk) {
+    const int nf = std::min(g.chunk, batch - b0);
+    launch_cols<kColBackward>(g, b0, nf, nullptr, 0.f, 0.f, 0.0, nullptr,
+                              const_cast<float2*>(reinterpret_cast<const float2*>(far_field)), nullptr, grad_output,
+                              s);
+    launch_rows_adjoint(g, S, P, positions_xy + 2 * (size_t)b0, nf, GS, GP, s);
+  }
+  return cuda_status(cudaGetLastError(), "ptx_base_backward launch");
+}
+
+int ptx_base_sweep(const float* sample, int sample_h, int sample_w, const float* probe, int probe_h, int probe_w,
+                   const int64_t* positions_xy, int batch, const uint16_t* measured, float scale, double* loss,
+                   float* grad_sample, float* grad_probe, void* workspace, size_t workspace_bytes, void* stream) {
+  BaseGeom g;
+  if (int st = check_common(sample, sample_h, sample_w, probe, probe_h, probe_w, positions_xy, batch, workspace,
+                            workspace_bytes, &g)) {
+    return st;
+  }
+  if (!measured || !loss || !grad_sample || !grad_probe) {
+    return set_error(PTX_ERR_INVALID_ARGUMENT, "null pointer argument");
+  }
+  if (!(scale > 0.f)) return set_error(PTX_ERR_INVALID_ARGUMENT, "scale must be positive");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  float2* GS = reinterpret_cast<float2*>(grad_sample);
+  float2* GP = reinterpret_cast<float2*>(grad_probe);
+  cudaMemsetAsync(GS, 0, sizeof(float2) * (size_t)sample_h * sample_w, s);
+  cudaMemsetAsync(GP, 0, sizeof(float2) * (size_t)probe_h * probe_w, s);
+  cudaMemsetAsync(loss, 0, sizeof(double), s);
+  cudaMemsetAsync(g.err, 0, sizeof(unsigned), s);
+  const double numel = (double)batch * probe_h * probe_w;
+  const float grad_scale = static_cast<float>(2.0 / std::max(numel, 1.0));
+  const float2* S = reinterpret_cast<const float2*>(sample);
+  const float2* P = reinterpret_cast<const float2*>(probe);
+  for (int b0 = 0; b0 < batch; b0 += g.chunk) {
+    const int nf = std::min(g.chunk, batch - b0);
+    const int64_t* pos = positions_xy + 2 * (size_t)b0;
+    launch_rows_forward(g, S, P, pos, nf, s);
+    launch_cols<kColSweep>(g, b0, nf, measured, scale, grad_scale, 1.0 / std::max(numel, 1.0), loss, nullptr,
+                           nullptr, nullptr, s);
+    launch_rows_adjoint(g, S, P, pos, nf, GS, GP, s);
+  }
+  return cuda_status(cudaGetLastError(), "ptx_base_sweep launch");
+}
+
+}  // extern "C"

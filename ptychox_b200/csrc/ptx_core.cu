@@ -1,0 +1,304 @@
+// Library core: error reporting, FFT line plans and their FP64-derived twiddle tables.
+//
+// The reference keeps a process-global cuFFT plan cache keyed by (device, batch, h, w)
+// behind a mutex (python/ptychoX/csrc/base_kernel.cu:19-91).  Here a "plan" is only the
+// radix sequence of one line length plus its twiddle table; tables live in a static
+// device pool (one per device), are filled once per (device, length) with a
+// synchronous copy, and are shared by every transform of that length.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <atomic>
+#include <map>
+#include <mutex>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "ptx_internal.h"
+
+namespace ptx {
+
+namespace {
+
+constexpr int kPoolEntries = 1 << 16;  // 512 KB of float2 per device
+__device__ float2 g_twiddle_pool[kPoolEntries];
+
+thread_local std::string g_last_error;
+
+std::mutex g_plan_mutex;
+std::map<int, int> g_table_offset;                       // n -> offset in the pool
+int g_pool_used = 0;
+std::map<std::pair<int, int>, LinePlan> g_plans;         // (device, n) -> plan
+
+bool factor_235(int n, int* a, int* b, int* c) {
+  *a = *b = *c = 0;
+  if (n < 2) return false;
+  while (n % 2 == 0) { n /= 2; ++*a; }
+  while (n % 3 == 0) { n /= 3; ++*b; }
+  while (n % 5 == 0) { n /= 5; ++*c; }
+  return n == 1;
+}
+
+// Radix sequence: the power-of-two part in ceil(a/4) balanced stages of radix 16/8/4/2,
+// then one stage per factor 3 and 5.
+int make_radices(int n, int* radix) {
+  int a, b, c;
+  if (!factor_235(n, &a, &b, &c)) return -1;
+  int ns = 0;
+  if (a > 0) {
+    const int stages = (a + 3) / 4;
+    int left = a;
+    for (int s = 0; s < stages; ++s) {
+      const int bits = (left + (stages - s) - 1) / (stages - s);  // ceil(left / remaining)
+      radix[ns++] = 1 << bits;
+      left -= bits;
+    }
+  }
+  for (int i = 0; i < b; ++i) radix[ns++] = 3;
+  for (int i = 0; i < c; ++i) radix[ns++] = 5;
+  return ns;
+}
+
+}  // namespace
+
+int set_error(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+int cuda_status(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return PTX_OK;
+  return set_error(PTX_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+bool size_supported(int n) {
+  int a, b, c;
+  if (n < 2 || n > 1024) return false;
+  if (!factor_235(n, &a, &b, &c)) return false;
+  int radix[kMaxStages];
+  return make_radices(n, radix) <= kMaxStages;
+}
+
+int get_line_plan(int n, LinePlan* out) {
+  if (!size_supported(n)) {
+    return set_error(PTX_ERR_UNSUPPORTED_SIZE,
+                     "transform length %d is not supported (needs 2^a 3^b 5^c, 2..1024)", n);
+  }
+  int dev = 0;
+  if (int st = cuda_status(cudaGetDevice(&dev), "cudaGetDevice")) return st;
+  std::lock_guard<std::mutex> lock(g_plan_mutex);
+  auto key = std::make_pair(dev, n);
+  auto it = g_plans.find(key);
+  if (it != g_plans.end()) {
+    *out = it->second;
+    return PTX_OK;
+  }
+  LinePlan p{};
+  p.n = n;
+  p.threads = (n + kValuesPerThread - 1) / kValuesPerThread;
+  int radix[kMaxStages];
+  p.nstages = make_radices(n, radix);
+  p.radices = 0;
+  for (int s = 0; s < p.nstages; ++s) p.radices |= static_cast<unsigned long long>(radix[s]) << (5 * s);
+  int offset;
+  auto ot = g_table_offset.find(n);
+  if (ot == g_table_offset.end()) {
+    if (g_pool_used + n > kPoolEntries) {
+      return set_error(PTX_ERR_UNSUPPORTED_SIZE, "twiddle pool exhausted (call ptx_clear_cache)");
+    }
+    offset = g_pool_used;
+    g_pool_used += (n + 31) / 32 * 32;
+    g_table_offset[n] = offset;
+  } else {
+    offset = ot->second;
+  }
+  std::vector<float2> table(n);
+  const double two_pi = 6.283185307179586476925286766559;
+  for (int m = 0; m < n; ++m) {
+    const double ang = two_pi * static_cast<double>(m) / static_cast<double>(n);
+    table[m] = make_float2(static_cast<float>(std::cos(ang)), static_cast<float>(-std::sin(ang)));
+  }
+  if (int st = cuda_status(cudaMemcpyToSymbol(g_twiddle_pool, table.data(), sizeof(float2) * n,
+                                              sizeof(float2) * offset, cudaMemcpyHostToDevice),
+                           "twiddle upload")) {
+    return st;
+  }
+  void* base = nullptr;
+  if (int st = cuda_status(cudaGetSymbolAddress(&base, g_twiddle_pool), "cudaGetSymbolAddress")) {
+    return st;
+  }
+  p.tw = reinterpret_cast<const float2*>(base) + offset;
+  g_plans[key] = p;
+  *out = p;
+  return PTX_OK;
+}
+
+int ensure_smem(const void* kernel, int bytes) {
+  if (bytes <= 48 * 1024) return PTX_OK;
+  return cuda_status(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
+                     "cudaFuncSetAttribute(MaxDynamicSharedMemorySize)");
+}
+
+RowShape row_shape(const LinePlan& p, int rows_available) {
+  RowShape s;
+  int lines = 256 / p.threads;
+  if (lines < 1) lines = 1;
+  if (lines > rows_available) lines = rows_available;
+  if (lines < 1) lines = 1;
+  s.lines = lines;
+  s.threads = ((lines * p.threads + 31) / 32) * 32;
+  s.smem = lines * line_pitch(p.n) * static_cast<int>(sizeof(float2));
+  return s;
+}
+
+ColShape col_shape(const LinePlan& p) {
+  ColShape s;
+  s.cols = kTile;
+  while (s.cols > 1 && s.cols * p.threads > 512) s.cols /= 2;
+  s.threads = ((s.cols * p.threads + 31) / 32) * 32;
+  s.smem = s.cols * line_pitch(p.n) * static_cast<int>(sizeof(float2));
+  return s;
+}
+
+namespace {
+const char* const kKernelNames[kNumKernelIds] = {
+    "base_rows_forward", "base_cols", "base_rows_adjoint", "fpm_rows_forward", "fpm_cols",
+    "fpm_rows_adjoint", "fft2_rows", "fft2_cols", "coded_rows", "coded_cols", "misc"};
+
+struct Profiler {
+  std::mutex mu;
+  bool on = false;
+  std::vector<cudaEvent_t> pool;
+  struct Pending { int id; cudaEvent_t a, b; };
+  std::vector<Pending> pending;
+  cudaEvent_t open_start[kNumKernelIds] = {};
+  double total_ms[kNumKernelIds] = {};
+  long long timed[kNumKernelIds] = {};
+};
+Profiler g_prof;
+std::atomic<long long> g_launches[kNumKernelIds];
+
+cudaEvent_t take_event() {
+  if (!g_prof.pool.empty()) {
+    cudaEvent_t e = g_prof.pool.back();
+    g_prof.pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+}  // namespace
+
+void prof_begin(int id, cudaStream_t s) {
+  g_launches[id].fetch_add(1, std::memory_order_relaxed);
+  if (!g_prof.on) return;
+  std::lock_guard<std::mutex> lock(g_prof.mu);
+  cudaEvent_t e = take_event();
+  cudaEventRecord(e, s);
+  g_prof.open_start[id] = e;
+}
+
+void prof_end(int id, cudaStream_t s) {
+  if (!g_prof.on) return;
+  std::lock_guard<std::mutex> lock(g_prof.mu);
+  if (!g_prof.open_start[id]) return;
+  cudaEvent_t e = take_event();
+  cudaEventRecord(e, s);
+  g_prof.pending.push_back({id, g_prof.open_start[id], e});
+  g_prof.open_start[id] = nullptr;
+}
+
+int sm_count() {
+  int dev = 0, n = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) {
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  }
+  return n > 0 ? n : 148;
+}
+
+}  // namespace ptx
+
+extern "C" {
+
+int ptx_version(void) { return 100; }  // 0.1.0
+
+const char* ptx_last_error(void) { return ptx::g_last_error.c_str(); }
+
+int ptx_clear_cache(void) {
+  std::lock_guard<std::mutex> lock(ptx::g_plan_mutex);
+  // Table offsets stay assigned: a table is rebuilt with identical contents at the same
+  // place, so kernels still in flight never see another length's table.
+  ptx::g_plans.clear();
+  return PTX_OK;
+}
+
+long long ptx_launch_count(void) {
+  long long n = 0;
+  for (int i = 0; i < ptx::kNumKernelIds; ++i) n += ptx::g_launches[i].load(std::memory_order_relaxed);
+  return n;
+}
+
+int ptx_profile_enable(int on) {
+  std::lock_guard<std::mutex> lock(ptx::g_prof.mu);
+  ptx::g_prof.on = on != 0;
+  return PTX_OK;
+}
+
+int ptx_profile_reset(void) {
+  std::lock_guard<std::mutex> lock(ptx::g_prof.mu);
+  for (auto& p : ptx::g_prof.pending) {
+    ptx::g_prof.pool.push_back(p.a);
+    ptx::g_prof.pool.push_back(p.b);
+  }
+  ptx::g_prof.pending.clear();
+  for (int i = 0; i < ptx::kNumKernelIds; ++i) {
+    ptx::g_prof.total_ms[i] = 0.0;
+    ptx::g_prof.timed[i] = 0;
+  }
+  return PTX_OK;
+}
+
+int ptx_profile_read(int kernel_id, double* total_ms, long long* launches) {
+  if (kernel_id < 0 || kernel_id >= ptx::kNumKernelIds || !total_ms || !launches) {
+    return ptx::set_error(PTX_ERR_INVALID_ARGUMENT, "bad kernel id");
+  }
+  std::lock_guard<std::mutex> lock(ptx::g_prof.mu);
+  for (auto& p : ptx::g_prof.pending) {
+    if (int st = ptx::cuda_status(cudaEventSynchronize(p.b), "cudaEventSynchronize")) return st;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, p.a, p.b);
+    ptx::g_prof.total_ms[p.id] += ms;
+    ptx::g_prof.timed[p.id] += 1;
+    ptx::g_prof.pool.push_back(p.a);
+    ptx::g_prof.pool.push_back(p.b);
+  }
+  ptx::g_prof.pending.clear();
+  *total_ms = ptx::g_prof.total_ms[kernel_id];
+  *launches = ptx::g_prof.timed[kernel_id];
+  return PTX_OK;
+}
+
+int ptx_profile_kinds(void) { return ptx::kNumKernelIds; }
+
+const char* ptx_profile_name(int kernel_id) {
+  if (kernel_id < 0 || kernel_id >= ptx::kNumKernelIds) return "";
+  return ptx::kKernelNames[kernel_id];
+}
+
+int ptx_fft_supported(int n) { return ptx::size_supported(n) ? 1 : 0; }
+
+int ptx_fft_prepare(int n) {
+  ptx::LinePlan p;
+  return ptx::get_line_plan(n, &p);
+}
+
+}  // extern "C"

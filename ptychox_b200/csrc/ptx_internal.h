@@ -1,0 +1,84 @@
+// Host-side internals shared by the translation units of libptychox.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include <string>
+#include <type_traits>
+
+#include "../../include/ptychox.h"
+#include "ptx_fft.cuh"
+
+namespace ptx {
+
+// Record an error message for ptx_last_error() and return `code`.
+int set_error(int code, const char* fmt, ...);
+// Map a CUDA error to PTX_ERR_CUDA with a message; returns PTX_OK for cudaSuccess.
+int cuda_status(cudaError_t e, const char* what);
+
+// Build (or fetch from the per-device cache) the line plan for length n on the current
+// device.  Returns PTX_OK or PTX_ERR_UNSUPPORTED_SIZE / PTX_ERR_CUDA.
+int get_line_plan(int n, LinePlan* out);
+bool size_supported(int n);
+
+// Enable large dynamic shared memory on a kernel once per device.
+int ensure_smem(const void* kernel, int bytes);
+
+inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Launch shapes shared by the pass kernels.
+struct RowShape {
+  int lines;    // lines (rows) per CTA
+  int threads;  // threads per CTA
+  int smem;     // dynamic shared memory bytes
+};
+RowShape row_shape(const LinePlan& p, int rows_available);
+struct ColShape {
+  int cols;     // columns per CTA (a divisor of kTile)
+  int threads;
+  int smem;
+};
+ColShape col_shape(const LinePlan& p);
+
+
+int sm_count();
+
+// Kernel kinds for the launch counter and the optional per-kernel event profiler.
+enum KernelId {
+  kBaseRowsForward = 0,
+  kBaseCols,
+  kBaseRowsAdjoint,
+  kFpmRowsForward,
+  kFpmCols,
+  kFpmRowsAdjoint,
+  kFft2Rows,
+  kFft2Cols,
+  kCodedRows,
+  kCodedCols,
+  kMiscKernel,
+  kNumKernelIds
+};
+// Call around every kernel launch: counts launches and, when profiling is on, records
+// a CUDA event pair on the launch stream.
+void prof_begin(int id, cudaStream_t s);
+void prof_end(int id, cudaStream_t s);
+
+// Line lengths that get compile-time FFT plans; every other supported length runs the
+// runtime-plan kernels (template argument 0).
+template <typename F>
+void dispatch_len(int n, F&& f) {
+  switch (n) {
+    case 16: f(std::integral_constant<int, 16>{}); return;
+    case 32: f(std::integral_constant<int, 32>{}); return;
+    case 64: f(std::integral_constant<int, 64>{}); return;
+    case 128: f(std::integral_constant<int, 128>{}); return;
+    case 256: f(std::integral_constant<int, 256>{}); return;
+    case 512: f(std::integral_constant<int, 512>{}); return;
+    case 1024: f(std::integral_constant<int, 1024>{}); return;
+    default: f(std::integral_constant<int, 0>{}); return;
+  }
+}
+
+}  // namespace ptx

@@ -1,0 +1,176 @@
+"""Conventional ptychography: CUDA library (through the C ABI) vs the oracle and golden vectors.
+
+Tolerance: relative L2 error ``||x - x_ref|| / ||x_ref||`` below 1e-5 for loss and
+gradients against the FP64 oracle / FP64 reference fixtures, the bar of the FP32 path.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import load_golden, rel_l2
+from oracle import ptycho_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+def cuda(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _lib():
+    import ptychox_b200  # noqa: F401
+    from ptychox_b200 import _abi
+
+    _abi.load()
+    assert torch.cuda.is_available()
+
+
+def run_sweep(sample, probe, pos, meas, scale):
+    from ptychox_b200.base import base_sweep
+
+    loss, gs, gp = base_sweep(cuda(sample), cuda(probe), cuda(pos.astype(np.int64)), cuda(meas), scale)
+    torch.cuda.synchronize()
+    return float(loss.item()), gs.cpu().numpy(), gp.cpu().numpy()
+
+
+def test_test_ops_case_forward_backward():
+    """python/test_ops.py:30-49 case (4x5 probe: runtime-plan kernels)."""
+    from ptychox_b200 import ptychoX_base
+
+    g = load_golden("test_ops_base.npz")
+    s = cuda(g["sample"]).requires_grad_(True)
+    p = cuda(g["probe"]).requires_grad_(True)
+    out = ptychoX_base(s, p, cuda(g["positions"]), use_cuda_kernels=True)
+    (out * cuda(g["grad"])).sum().backward()
+    assert rel_l2(out.detach().cpu().numpy(), g["out"]) < TOL
+    assert rel_l2(s.grad.cpu().numpy(), g["grad_sample"]) < TOL
+    assert rel_l2(p.grad.cpu().numpy(), g["grad_probe"]) < TOL
+
+
+@pytest.mark.parametrize("name", ["sweep_base_fp64.npz", "sweep_base_odd_fp64.npz"])
+def test_sweep_golden(name):
+    g = load_golden(name)
+    loss, gs, gp = run_sweep(g["sample"], g["probe"], g["positions"], g["measured"], float(g["scale"]))
+    assert abs(loss - float(g["loss"])) <= TOL * abs(float(g["loss"]))
+    assert rel_l2(gs, g["grad_sample"]) < TOL
+    assert rel_l2(gp, g["grad_probe"]) < TOL
+
+
+def small_problem(n_obj, p, grid, step, origin, jitter, photons, seed):
+    from ptychox_b200 import synth
+
+    rng = np.random.default_rng(seed)
+    obj = synth.random_object(n_obj, n_obj, rng)
+    probe = synth.gaussian_probe(p, p, rng)
+    pos = synth.raster_positions(grid, step, origin, jitter, rng)
+    amp, _, _ = O.base_forward(obj, probe, pos)
+    meas, scale = synth.poisson_counts(amp**2, photons, rng)
+    guess = (obj * (1 + 0.1 * rng.standard_normal(obj.shape))).astype(np.complex64)
+    return guess, probe, pos, meas, scale
+
+
+@pytest.mark.parametrize("p", [32, 64, 96, 128, 160])
+def test_sweep_vs_oracle_sizes(p):
+    """Compile-time (32, 64, 128) and runtime-plan (96, 160) transform lengths."""
+    obj, probe, pos, meas, scale = small_problem(4 * p, p, 4, p // 2, 3, 2, 1e4, seed=p)
+    loss, gs, gp = run_sweep(obj, probe, pos, meas, scale)
+    rl, rs, rp = O.base_sweep(obj, probe, pos, meas, scale)
+    assert abs(loss - rl) <= TOL * abs(rl)
+    assert rel_l2(gs, rs) < TOL
+    assert rel_l2(gp, rp) < TOL
+
+
+def test_config0_sweep_vs_oracle():
+    """Config 0 shape: 512x512 object, 128x128 probe, 11x11 raster step 32 with U[-2,2] jitter."""
+    obj, probe, pos, meas, scale = small_problem(512, 128, 11, 32, 8, 2, 1e4, seed=0)
+    loss, gs, gp = run_sweep(obj, probe, pos, meas, scale)
+    rl, rs, rp = O.base_sweep(obj, probe, pos, meas, scale)
+    assert abs(loss - rl) <= TOL * abs(rl)
+    assert rel_l2(gs, rs) < TOL
+    assert rel_l2(gp, rp) < TOL
+
+
+def test_operator_matches_oracle_and_fused():
+    """autograd.Function forward/backward vs the oracle, and vs the fused sweep."""
+    from ptychox_b200 import ptychoX_base, ptychoX_base_loss
+
+    obj, probe, pos, meas, scale = small_problem(256, 64, 5, 40, 4, 2, 1e4, seed=3)
+    rng = np.random.default_rng(5)
+    gout = rng.standard_normal((len(pos), 64, 64)).astype(np.float32)
+    s = cuda(obj).requires_grad_(True)
+    p = cuda(probe).requires_grad_(True)
+    amp = ptychoX_base(s, p, torch.from_numpy(pos))  # CPU positions are accepted
+    (amp * cuda(gout)).sum().backward()
+    ramp, far, patches = O.base_forward(obj, probe, pos)
+    rgs, rgp = O.base_backward(gout, patches, probe.astype(np.complex128), far, pos, obj.shape)
+    assert rel_l2(amp.detach().cpu().numpy(), ramp) < TOL
+    assert rel_l2(s.grad.cpu().numpy(), rgs) < TOL
+    assert rel_l2(p.grad.cpu().numpy(), rgp) < TOL
+
+    s2 = cuda(obj).requires_grad_(True)
+    p2 = cuda(probe).requires_grad_(True)
+    amp2 = ptychoX_base(s2, p2, cuda(pos))
+    observed = torch.sqrt(cuda(meas).to(torch.float32) * np.float32(scale))
+    torch.nn.functional.mse_loss(amp2, observed).backward()
+    s3 = cuda(obj).requires_grad_(True)
+    p3 = cuda(probe).requires_grad_(True)
+    ptychoX_base_loss(s3, p3, cuda(pos), cuda(meas), scale).backward()
+    assert rel_l2(s3.grad.cpu().numpy(), s2.grad.cpu().numpy()) < TOL
+    assert rel_l2(p3.grad.cpu().numpy(), p2.grad.cpu().numpy()) < TOL
+
+
+def test_chunked_workspace_matches():
+    """A workspace holding one frame (many launches) gives the same result as a full one."""
+    from ptychox_b200 import _abi
+    from ptychox_b200.base import base_sweep
+
+    obj, probe, pos, meas, scale = small_problem(256, 64, 5, 40, 4, 2, 1e4, seed=4)
+    full = base_sweep(cuda(obj), cuda(probe), cuda(pos), cuda(meas), scale)
+    frame = 64 * 64 * 8
+    ws = torch.empty(256 + frame, dtype=torch.uint8, device="cuda")
+    one = base_sweep(cuda(obj), cuda(probe), cuda(pos), cuda(meas), scale, ws=ws)
+    assert abs(float(full[0]) - float(one[0])) <= 1e-12 * abs(float(full[0]))
+    assert rel_l2(one[1].cpu().numpy(), full[1].cpu().numpy()) < 1e-6
+    with pytest.raises(RuntimeError):
+        base_sweep(cuda(obj), cuda(probe), cuda(pos), cuda(meas), scale,
+                   ws=torch.empty(frame // 2, dtype=torch.uint8, device="cuda"))
+    assert _abi.query("ptx_fft_supported", 7) == 0
+
+
+def test_errors_are_mapped():
+    from ptychox_b200 import ptychoX_base
+
+    s = torch.zeros(64, 64, dtype=torch.complex64, device="cuda")
+    p = torch.zeros(14, 14, dtype=torch.complex64, device="cuda")  # 14 = 2*7: unsupported length
+    with pytest.raises(ValueError):
+        ptychoX_base(s, p, torch.zeros(1, 2, dtype=torch.long))
+    p = torch.zeros(16, 16, dtype=torch.complex64, device="cuda")
+    with pytest.raises(ValueError):
+        ptychoX_base(s, p, torch.tensor([[60, 0]]))  # window leaves the sample
+    with pytest.raises(TypeError):
+        ptychoX_base(s.to(torch.complex128), p.to(torch.complex128), torch.zeros(1, 2, dtype=torch.long))
+    out = ptychoX_base(s, p, torch.zeros(0, 2, dtype=torch.long))
+    assert out.shape == (0, 16, 16)
+
+
+def test_config1_subset_vs_oracle():
+    """Config 1 frame size (2048^2 object, 512^2 probe) on a 48-position subset vs FP64 oracle."""
+    from ptychox_b200 import synth
+
+    rng = np.random.default_rng(1)
+    obj = synth.random_object(2048, 2048, rng)
+    probe = synth.gaussian_probe(512, 512, rng)
+    pos = synth.raster_positions(30, 48, 64, 3, rng)
+    sub = pos[rng.choice(len(pos), 48, replace=False)]
+    amp, _, _ = O.base_forward(obj, probe, sub, fp64=False)
+    meas, scale = synth.poisson_counts(amp.astype(np.float64) ** 2, 1e5, rng)
+    guess = (obj * (1 + 0.1 * rng.standard_normal(obj.shape))).astype(np.complex64)
+    loss, gs, gp = run_sweep(guess, probe, sub, meas, scale)
+    rl, rs, rp = O.base_sweep(guess, probe, sub, meas, scale)
+    assert abs(loss - rl) <= TOL * abs(rl)
+    assert rel_l2(gs, rs) < TOL
+    assert rel_l2(gp, rp) < TOL
