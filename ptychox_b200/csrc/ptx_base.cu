@@ -17,14 +17,16 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "ptx_internal.h"
+#include "ptx_regfft.cuh"
 
 namespace ptx {
 namespace {
 
 constexpr size_t kHeaderBytes = 256;           // error word + padding
-constexpr size_t kTargetScratch = 64u << 20;   // frames per launch sized to ~L2
+constexpr size_t kTargetScratch = 4096ull << 20;  // upper bound on workspace frames
 constexpr float kEps = 1.1920928955078125e-07f;  // torch.finfo(float32).eps
 
 enum ColMode { kColSweep = 0, kColForward = 1, kColBackward = 2 };
@@ -35,7 +37,7 @@ __device__ __forceinline__ bool window_ok(long long x0, long long y0, int ph, in
 
 // Row pass 1: gather O rows, multiply by the probe, forward row DFT, store tiled.
 template <int NR>
-__global__ void __launch_bounds__(256) base_rows_forward(
+__global__ void __launch_bounds__(256) base_rows_forward_rt(
     const float2* __restrict__ sample, int H, int W, const float2* __restrict__ probe, int ph, int pw,
     const int64_t* __restrict__ pos, int nframes, int frames_per_cta, float2* __restrict__ scratch,
     LinePlan plan, int lines, unsigned* __restrict__ err) {
@@ -79,7 +81,7 @@ __global__ void __launch_bounds__(256) base_rows_forward(
 // kColForward: column DFT, write fftshifted far field and amplitude.
 // kColBackward: build g F/|F| from the saved far field, inverse column DFT.
 template <int MODE, int NC>
-__global__ void __launch_bounds__(512, 1) base_cols(
+__global__ void __launch_bounds__(512, 1) base_cols_rt(
     float2* __restrict__ scratch, int ph, int pw, int frame0, LinePlan plan, int cols,
     const uint16_t* __restrict__ measured, float scale, float grad_scale, double inv_numel,
     double* __restrict__ loss, float2* __restrict__ far_field, float* __restrict__ amplitude,
@@ -179,7 +181,7 @@ __global__ void __launch_bounds__(512, 1) base_cols(
 constexpr int kOwn = kValuesPerThread;  // elements of a line owned by one thread
 
 template <int NR>
-__global__ void __launch_bounds__(256) base_rows_adjoint(
+__global__ void __launch_bounds__(256) base_rows_adjoint_rt(
     const float2* __restrict__ scratch, const float2* __restrict__ sample, int H, int W,
     const float2* __restrict__ probe, int ph, int pw, const int64_t* __restrict__ pos, int nframes,
     int frames_per_cta, float2* __restrict__ grad_sample, float2* __restrict__ grad_probe,
@@ -244,6 +246,275 @@ __global__ void __launch_bounds__(256) base_rows_adjoint(
   }
 }
 
+
+// ---------------------------------------------------------------------------------------
+// Register-FFT kernels for power-of-two line lengths (the hot sizes).  Each thread keeps
+// RegShape<N>::N1 values of its line in registers from the global load to the global
+// store; one shared-memory transpose per 1-D transform.
+// ---------------------------------------------------------------------------------------
+
+template <int N>
+struct RowCfg {
+  static constexpr int T = RegShape<N>::T;
+  static constexpr int LP = row_line_pitch<N>();
+};
+
+// Row pass 1 (register FFT): gather O rows x probe rows, forward row DFT, store tiled.
+template <int N>
+__global__ void __launch_bounds__(256, 2) base_rows_forward_reg(
+    const float2* __restrict__ sample, int H, int W, const float2* __restrict__ probe, int ph,
+    const int64_t* __restrict__ pos, float2* __restrict__ scratch, const float2* __restrict__ tw, int lines,
+    unsigned* __restrict__ err) {
+  using S = RegShape<N>;
+  constexpr int kTiles = N / kTile;
+  extern __shared__ float2 sm[];
+  const int tid = threadIdx.x;
+  const int l = tid / S::T;
+  const int t = tid - l * S::T;
+  const int r = blockIdx.x * lines + l;
+  const int f = blockIdx.y;
+  const bool row_ok = r < ph;
+  const long long x0 = pos[2 * f], y0 = pos[2 * f + 1];
+  const bool ok = window_ok(x0, y0, ph, N, H, W);
+  if (!ok && tid == 0 && blockIdx.x == 0) atomicOr(err, 1u);
+  float2 v[S::N1];
+  if (ok && row_ok) {
+    const float2* orow = sample + (y0 + r) * W + x0;
+    const float2* prow = probe + (size_t)r * N;
+#pragma unroll
+    for (int j = 0; j < S::N1; ++j) {
+      const int c = t + S::T * j;
+      v[j] = cmul(orow[c], __ldg(&prow[c]));
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < S::N1; ++j) v[j] = make_float2(0.f, 0.f);
+  }
+  reg_fft<N, false, false>(v, sm + l * RowCfg<N>::LP, t, tw);
+  if (row_ok) {
+    float2* base = scratch + (size_t)f * kTiles * ph * kTile + (size_t)r * kTile;
+#pragma unroll
+    for (int m = 0; m < S::N1; ++m) {
+      const int kc = t + S::T * m;
+      base[(size_t)(kc / kTile) * ph * kTile + (kc % kTile)] = v[m];
+    }
+  }
+}
+
+// Column pass (register FFT), same three modes as base_cols_rt.  A CTA owns kColsReg
+// columns of one frame; threads run column-fastest (thread (t, c) owns column c).  In
+// the sweep mode the uint16 counts of the CTA's columns are prefetched into shared
+// memory with cp.async before the forward column DFT, so their latency hides behind it.
+constexpr int kColsReg = 8;
+
+template <int N>
+struct ColCfg {
+  static constexpr int LP = col_line_pitch<N>();
+  static constexpr int kMeasOffsetBytes = ((kColsReg * LP * (int)sizeof(float2)) + 15) / 16 * 16;
+  static constexpr int kSmemBytes = kMeasOffsetBytes + N * kColsReg * (int)sizeof(uint16_t);
+};
+
+template <int MODE, int N>
+__global__ void __launch_bounds__(256, 2) base_cols_reg(
+    float2* __restrict__ scratch, int pw, int frame0, const float2* __restrict__ tw,
+    const uint16_t* __restrict__ measured, float scale, float grad_scale, double inv_numel,
+    double* __restrict__ loss, float2* __restrict__ far_field, float* __restrict__ amplitude,
+    const float* __restrict__ grad_output) {
+  using S = RegShape<N>;
+  constexpr int LP = ColCfg<N>::LP;
+  extern __shared__ float2 sm[];
+  __shared__ double red[32];
+  uint16_t* meas_s = reinterpret_cast<uint16_t*>(reinterpret_cast<char*>(sm) + ColCfg<N>::kMeasOffsetBytes);
+  const int tid = threadIdx.x;
+  const int c = tid % kColsReg;
+  const int t = tid / kColsReg;
+  constexpr int kSubs = kTile / kColsReg;
+  const int ct = blockIdx.x / kSubs;
+  const int c0 = ct * kTile + (blockIdx.x - ct * kSubs) * kColsReg;  // first column of the CTA
+  const int f = blockIdx.y;
+  const int kc = c0 + c;
+  const bool col_ok = kc < pw;
+  const int tiles = num_tiles(pw);
+  float2* tile = scratch + ((size_t)f * tiles + ct) * N * kTile + (c0 - ct * kTile);
+  const size_t g = (size_t)frame0 + f;
+  float2* buf = sm + c * LP;
+  int ic = kc + pw / 2;
+  if (ic >= pw) ic -= pw;
+  float2 v[S::N1];
+
+  if (MODE == kColSweep) {
+    // counts of rows kr (unshifted) -> meas_s[kr][c]
+    int ic0 = c0 + pw / 2;
+    if (ic0 >= pw) ic0 -= pw;
+    const bool fast = (pw % (2 * kColsReg) == 0) && ((reinterpret_cast<uintptr_t>(measured) & 15) == 0);
+    if (fast) {
+      for (int kr = tid; kr < N; kr += blockDim.x) {
+        const int ir = (kr + N / 2) & (N - 1);
+        cp_async16(meas_s + kr * kColsReg, measured + (g * N + ir) * pw + ic0);
+      }
+      cp_async_commit();
+    } else {
+      for (int i = tid; i < N * kColsReg; i += blockDim.x) {
+        const int kr = i / kColsReg, cc = i - kr * kColsReg;
+        const int ir = (kr + N / 2) & (N - 1);
+        int icc = c0 + cc + pw / 2;
+        if (icc >= pw) icc -= pw;
+        meas_s[i] = (c0 + cc < pw) ? measured[(g * N + ir) * pw + icc] : 0;
+      }
+    }
+  }
+
+  if (MODE != kColBackward) {
+#pragma unroll
+    for (int j = 0; j < S::N1; ++j) {
+      v[j] = col_ok ? tile[(t + S::T * j) * kTile + c] : make_float2(0.f, 0.f);
+    }
+    reg_fft<N, false, true>(v, buf, t, tw);
+  }
+
+  if (MODE == kColSweep) {
+    cp_async_wait_all();
+    __syncthreads();
+    double acc = 0.0;
+#pragma unroll
+    for (int m = 0; m < S::N1; ++m) {
+      const int kr = t + S::T * m;
+      const float2 F = v[m];
+      float2 out = make_float2(0.f, 0.f);
+      if (col_ok) {
+        const float y = sqrtf(static_cast<float>(meas_s[kr * kColsReg + c]) * scale);
+        const float a = cabsf(F);
+        const float rr = a - y;
+        acc += static_cast<double>(rr) * static_cast<double>(rr);
+        out = cscale(F, grad_scale * rr / fmaxf(a, kEps));
+      }
+      v[m] = out;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((tid & 31) == 0) red[tid >> 5] = acc;
+    __syncthreads();
+    if (tid < 32) {
+      const int nw = (blockDim.x + 31) >> 5;
+      double w = (tid < nw) ? red[tid] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+      if (tid == 0) atomicAdd(loss, w * inv_numel);
+    }
+  } else if (MODE == kColForward) {
+    if (col_ok) {
+#pragma unroll
+      for (int m = 0; m < S::N1; ++m) {
+        const int kr = t + S::T * m;
+        const int ir = (kr + N / 2) & (N - 1);
+        const size_t idx = (g * N + ir) * pw + ic;
+        if (far_field) far_field[idx] = v[m];
+        amplitude[idx] = cabsf(v[m]);
+      }
+    }
+    return;
+  } else {  // kColBackward
+#pragma unroll
+    for (int m = 0; m < S::N1; ++m) {
+      const int kr = t + S::T * m;
+      const int ir = (kr + N / 2) & (N - 1);
+      float2 out = make_float2(0.f, 0.f);
+      if (col_ok) {
+        const size_t idx = (g * N + ir) * pw + ic;
+        const float2 F = far_field[idx];
+        out = cscale(F, grad_output[idx] / fmaxf(cabsf(F), kEps));
+      }
+      v[m] = out;
+    }
+  }
+  reg_fft<N, true, true>(v, buf, t, tw);
+  if (col_ok) {
+#pragma unroll
+    for (int m = 0; m < S::N1; ++m) tile[(t + S::T * m) * kTile + c] = v[m];
+  }
+}
+
+// Row pass 2 (register FFT): inverse row DFT, scatter G conj(P) into grad_O, accumulate
+// G conj(O) for grad_P in registers across this CTA's frames.
+template <int N>
+__global__ void __launch_bounds__(128, 3) base_rows_adjoint_reg(
+    const float2* __restrict__ scratch, const float2* __restrict__ sample, int H, int W,
+    const float2* __restrict__ probe, int ph, const int64_t* __restrict__ pos, int nframes, int frames_per_cta,
+    float2* __restrict__ grad_sample, float2* __restrict__ grad_probe, const float2* __restrict__ tw, int lines) {
+  using S = RegShape<N>;
+  constexpr int kTiles = N / kTile;
+  extern __shared__ float2 sm[];
+  const int tid = threadIdx.x;
+  const int l = tid / S::T;
+  const int t = tid - l * S::T;
+  const int r = blockIdx.x * lines + l;
+  const bool row_ok = r < ph;
+  const int f0 = blockIdx.y * frames_per_cta;
+  const int f1 = min(nframes, f0 + frames_per_cta);
+  float2* buf = sm + l * RowCfg<N>::LP;
+  // this line's object row, prefetched with cp.async (each thread copies and later reads
+  // exactly the elements it owns, so only its own copies need waiting for)
+  float2* obuf = sm + lines * RowCfg<N>::LP + l * N;
+  const float2* prow = probe + (size_t)(row_ok ? r : 0) * N;
+  float2 acc[S::N1];
+#pragma unroll
+  for (int m = 0; m < S::N1; ++m) acc[m] = make_float2(0.f, 0.f);
+  for (int f = f0; f < f1; ++f) {
+    const long long x0 = pos[2 * f], y0 = pos[2 * f + 1];
+    const bool ok = window_ok(x0, y0, ph, N, H, W);
+    if (row_ok && ok) {
+      const float2* orow = sample + (y0 + r) * W + x0;
+#pragma unroll
+      for (int m = 0; m < S::N1; ++m) cp_async8(obuf + t + S::T * m, orow + t + S::T * m);
+      cp_async_commit();
+    }
+    float2 v[S::N1];
+    if (row_ok) {
+      const float2* base = scratch + (size_t)f * kTiles * ph * kTile + (size_t)r * kTile;
+#pragma unroll
+      for (int j = 0; j < S::N1; ++j) {
+        const int c = t + S::T * j;
+        v[j] = base[(size_t)(c / kTile) * ph * kTile + (c % kTile)];
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < S::N1; ++j) v[j] = make_float2(0.f, 0.f);
+    }
+    reg_fft<N, true, false>(v, buf, t, tw);
+    if (row_ok && ok) {
+      float2* grow = grad_sample + (y0 + r) * W + x0;
+      cp_async_wait_all();
+#pragma unroll
+      for (int m = 0; m < S::N1; ++m) {
+        const int c = t + S::T * m;
+        const float2 G = v[m];
+        atomicAdd(&grow[c], cmulc(G, __ldg(&prow[c])));
+        acc[m] = cadd(acc[m], cmulc(G, obuf[c]));
+      }
+    }
+  }
+  if (row_ok) {
+#pragma unroll
+    for (int m = 0; m < S::N1; ++m) atomicAdd(&grad_probe[(size_t)r * N + t + S::T * m], acc[m]);
+  }
+}
+
+template <int N>
+struct RegLaunch {
+  static constexpr int T = RegShape<N>::T;
+  // rows per CTA (multiple of 32 / T so the block is whole warps)
+  static int lines(int threads, int ph) {
+    int l = threads / T;
+    const int quantum = T >= 32 ? 1 : 32 / T;
+    const int need = ((ph + quantum - 1) / quantum) * quantum;
+    return l < need ? l : need;
+  }
+  static int row_smem(int lines) { return lines * RowCfg<N>::LP * (int)sizeof(float2); }
+  static int adj_smem(int lines) { return lines * (RowCfg<N>::LP + N) * (int)sizeof(float2); }
+  static int col_threads() { return kColsReg * T; }
+  static int col_smem() { return ColCfg<N>::kSmemBytes; }
+};
+
 struct BaseGeom {
   int H, W, ph, pw, batch;
   LinePlan row, col;
@@ -276,21 +547,38 @@ int check_common(const void* sample, int H, int W, const void* probe, int ph, in
     return set_error(PTX_ERR_WORKSPACE, "workspace of %zu bytes is smaller than one frame (%zu)",
                      ws_bytes, kHeaderBytes + g->frame_bytes);
   }
-  const size_t fit = (ws_bytes - kHeaderBytes) / g->frame_bytes;
+  size_t fit = (ws_bytes - kHeaderBytes) / g->frame_bytes;
+  if (const char* env = getenv("PTYCHOX_CHUNK_FRAMES")) {
+    const long v = atol(env);
+    if (v > 0 && (size_t)v < fit) fit = (size_t)v;
+  }
   g->chunk = static_cast<int>(std::min<size_t>(fit, (size_t)std::max(batch, 1)));
   g->err = reinterpret_cast<unsigned*>(ws);
   g->scratch = reinterpret_cast<float2*>(static_cast<char*>(ws) + kHeaderBytes);
   int st = PTX_OK;
   dispatch_len(pw, [&](auto NT) {
     constexpr int N = decltype(NT)::value;
-    if (!st) st = ensure_smem((const void*)base_rows_forward<N>, g->rs.smem);
-    if (!st) st = ensure_smem((const void*)base_rows_adjoint<N>, g->rs.smem);
+    if constexpr (N > 0) {
+      using L = RegLaunch<N>;
+      if (!st) st = ensure_smem((const void*)base_rows_forward_reg<N>, L::row_smem(L::lines(256, ph)));
+      if (!st) st = ensure_smem((const void*)base_rows_adjoint_reg<N>, L::adj_smem(L::lines(128, ph)));
+    } else {
+      if (!st) st = ensure_smem((const void*)base_rows_forward_rt<0>, g->rs.smem);
+      if (!st) st = ensure_smem((const void*)base_rows_adjoint_rt<0>, g->rs.smem);
+    }
   });
   dispatch_len(ph, [&](auto NT) {
     constexpr int N = decltype(NT)::value;
-    if (!st) st = ensure_smem((const void*)base_cols<kColSweep, N>, g->cs.smem);
-    if (!st) st = ensure_smem((const void*)base_cols<kColForward, N>, g->cs.smem);
-    if (!st) st = ensure_smem((const void*)base_cols<kColBackward, N>, g->cs.smem);
+    if constexpr (N > 0) {
+      const int sm = RegLaunch<N>::col_smem();
+      if (!st) st = ensure_smem((const void*)base_cols_reg<kColSweep, N>, sm);
+      if (!st) st = ensure_smem((const void*)base_cols_reg<kColForward, N>, sm);
+      if (!st) st = ensure_smem((const void*)base_cols_reg<kColBackward, N>, sm);
+    } else {
+      if (!st) st = ensure_smem((const void*)base_cols_rt<kColSweep, 0>, g->cs.smem);
+      if (!st) st = ensure_smem((const void*)base_cols_rt<kColForward, 0>, g->cs.smem);
+      if (!st) st = ensure_smem((const void*)base_cols_rt<kColBackward, 0>, g->cs.smem);
+    }
   });
   if (st) return st;
   return PTX_OK;
@@ -304,28 +592,46 @@ int frames_per_cta_for(int rowgroups, int nframes, int target_ctas) {
 
 void launch_rows_forward(const BaseGeom& g, const float2* sample, const float2* probe, const int64_t* pos,
                          int nframes, cudaStream_t s) {
-  const int rowgroups = (g.ph + g.rs.lines - 1) / g.rs.lines;
-  dim3 grid(rowgroups, nframes);
   prof_begin(kBaseRowsForward, s);
   dispatch_len(g.pw, [&](auto NT) {
     constexpr int N = decltype(NT)::value;
-    base_rows_forward<N><<<grid, g.rs.threads, g.rs.smem, s>>>(sample, g.H, g.W, probe, g.ph, g.pw, pos,
-                                                               nframes, 1, g.scratch, g.row, g.rs.lines, g.err);
+    if constexpr (N > 0) {
+      using L = RegLaunch<N>;
+      const int lines = L::lines(256, g.ph);
+      dim3 grid((g.ph + lines - 1) / lines, nframes);
+      base_rows_forward_reg<N><<<grid, lines * L::T, L::row_smem(lines), s>>>(sample, g.H, g.W, probe, g.ph, pos,
+                                                                             g.scratch, g.row.tw, lines, g.err);
+    } else {
+      const int rowgroups = (g.ph + g.rs.lines - 1) / g.rs.lines;
+      dim3 grid(rowgroups, nframes);
+      base_rows_forward_rt<0><<<grid, g.rs.threads, g.rs.smem, s>>>(sample, g.H, g.W, probe, g.ph, g.pw, pos,
+                                                                    nframes, 1, g.scratch, g.row, g.rs.lines, g.err);
+    }
   });
   prof_end(kBaseRowsForward, s);
 }
 
 void launch_rows_adjoint(const BaseGeom& g, const float2* sample, const float2* probe, const int64_t* pos,
                          int nframes, float2* grad_sample, float2* grad_probe, cudaStream_t s) {
-  const int rowgroups = (g.ph + g.rs.lines - 1) / g.rs.lines;
-  const int fpc = frames_per_cta_for(rowgroups, nframes, sm_count() * 8);
-  dim3 grid(rowgroups, (nframes + fpc - 1) / fpc);
   prof_begin(kBaseRowsAdjoint, s);
   dispatch_len(g.pw, [&](auto NT) {
     constexpr int N = decltype(NT)::value;
-    base_rows_adjoint<N><<<grid, g.rs.threads, g.rs.smem, s>>>(g.scratch, sample, g.H, g.W, probe, g.ph, g.pw,
-                                                               pos, nframes, fpc, grad_sample, grad_probe, g.row,
-                                                               g.rs.lines);
+    if constexpr (N > 0) {
+      using L = RegLaunch<N>;
+      const int lines = L::lines(128, g.ph);
+      const int rowgroups = (g.ph + lines - 1) / lines;
+      const int fpc = frames_per_cta_for(rowgroups, nframes, sm_count() * 6);
+      dim3 grid(rowgroups, (nframes + fpc - 1) / fpc);
+      base_rows_adjoint_reg<N><<<grid, lines * L::T, L::adj_smem(lines), s>>>(
+          g.scratch, sample, g.H, g.W, probe, g.ph, pos, nframes, fpc, grad_sample, grad_probe, g.row.tw, lines);
+    } else {
+      const int rowgroups = (g.ph + g.rs.lines - 1) / g.rs.lines;
+      const int fpc = frames_per_cta_for(rowgroups, nframes, sm_count() * 8);
+      dim3 grid(rowgroups, (nframes + fpc - 1) / fpc);
+      base_rows_adjoint_rt<0><<<grid, g.rs.threads, g.rs.smem, s>>>(g.scratch, sample, g.H, g.W, probe, g.ph,
+                                                                    g.pw, pos, nframes, fpc, grad_sample,
+                                                                    grad_probe, g.row, g.rs.lines);
+    }
   });
   prof_end(kBaseRowsAdjoint, s);
 }
@@ -334,13 +640,22 @@ template <int MODE>
 void launch_cols(const BaseGeom& g, int frame0, int nframes, const uint16_t* measured, float scale,
                  float grad_scale, double inv_numel, double* loss, float2* far_field, float* amplitude,
                  const float* grad_output, cudaStream_t s) {
-  dim3 grid(num_tiles(g.pw) * (kTile / g.cs.cols), nframes);
   prof_begin(kBaseCols, s);
   dispatch_len(g.ph, [&](auto NT) {
     constexpr int N = decltype(NT)::value;
-    base_cols<MODE, N><<<grid, g.cs.threads, g.cs.smem, s>>>(g.scratch, g.ph, g.pw, frame0, g.col, g.cs.cols,
-                                                             measured, scale, grad_scale, inv_numel, loss,
-                                                             far_field, amplitude, grad_output);
+    if constexpr (N > 0) {
+      using L = RegLaunch<N>;
+      dim3 grid(num_tiles(g.pw) * (kTile / kColsReg), nframes);
+      base_cols_reg<MODE, N><<<grid, L::col_threads(), L::col_smem(), s>>>(
+          g.scratch, g.pw, frame0, g.col.tw, measured, scale, grad_scale, inv_numel, loss, far_field, amplitude,
+          grad_output);
+    } else {
+      dim3 grid(num_tiles(g.pw) * (kTile / g.cs.cols), nframes);
+      base_cols_rt<MODE, 0><<<grid, g.cs.threads, g.cs.smem, s>>>(g.scratch, g.ph, g.pw, frame0, g.col,
+                                                                  g.cs.cols, measured, scale, grad_scale,
+                                                                  inv_numel, loss, far_field, amplitude,
+                                                                  grad_output);
+    }
   });
   prof_end(kBaseCols, s);
 }
@@ -368,7 +683,7 @@ int ptx_base_forward(const float* sample, int sample_h, int sample_w, const floa
                             workspace_bytes, &g)) {
     return st;
   }
-  if (!amplitude) return set_error(PTX_ERR_INVALID_ARGUMENT, "amplitude is null");
+  if (!amplitude && batch > 0) return set_error(PTX_ERR_INVALID_ARGUMENT, "amplitude is null");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   cudaMemsetAsync(g.err, 0, sizeof(unsigned), s);
   const float2* S = reinterpret_cast<const float2*>(sample);
@@ -391,7 +706,7 @@ int ptx_base_backward(const float* grad_output, const float* far_field, const fl
                             workspace_bytes, &g)) {
     return st;
   }
-  if (!grad_output || !far_field || !grad_sample || !grad_probe) {
+  if (((!grad_output || !far_field) && batch > 0) || !grad_sample || !grad_probe) {
     return set_error(PTX_ERR_INVALID_ARGUMENT, "null pointer argument");
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -419,7 +734,7 @@ int ptx_base_sweep(const float* sample, int sample_h, int sample_w, const float*
                             workspace_bytes, &g)) {
     return st;
   }
-  if (!measured || !loss || !grad_sample || !grad_probe) {
+  if ((!measured && batch > 0) || !loss || !grad_sample || !grad_probe) {
     return set_error(PTX_ERR_INVALID_ARGUMENT, "null pointer argument");
   }
   if (!(scale > 0.f)) return set_error(PTX_ERR_INVALID_ARGUMENT, "scale must be positive");
