@@ -115,6 +115,24 @@ int ptx_base_sweep(const float* sample, int sample_h, int sample_w,
                    double* loss, float* grad_sample, float* grad_probe,
                    void* workspace, size_t workspace_bytes, void* stream);
 
+/* Allocation-free fused sweep, for callers that cannot allocate device memory: a host
+ * program that loads this library as a plug-in and keeps the GPU memory pool to itself,
+ * or an acquisition loop that must not take the device-wide synchronisation of a
+ * cudaMalloc/cudaFree mid-scan.  No counterpart in the reference (which allocates every
+ * temporary with torch::empty / torch::zeros, base_kernel.cu:250-251,281-282).
+ * Same arguments and results as ptx_base_sweep minus the workspace: the scratch frames
+ * live in a fixed PTX_NOALLOC_SCRATCH_BYTES device array that every GPU loading the
+ * library holds until exit.  A probe frame (width rounded up to 16) times 8 bytes plus
+ * 256 must fit in it, else PTX_ERR_WORKSPACE.  The first call on a device looks up the
+ * array's device address (make it before any CUDA graph capture).  All calls share the
+ * array: calls that overlap on the GPU race and must be serialised by the caller. */
+#define PTX_NOALLOC_SCRATCH_BYTES (8u * 1024u * 1024u)
+int ptx_base_sweep_noalloc(const float* sample, int sample_h, int sample_w,
+                           const float* probe, int probe_h, int probe_w,
+                           const int64_t* positions_xy, int batch,
+                           const uint16_t* measured, float scale,
+                           double* loss, float* grad_sample, float* grad_probe, void* stream);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif
