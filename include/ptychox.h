@@ -115,6 +115,42 @@ int ptx_base_sweep(const float* sample, int sample_h, int sample_w,
                    double* loss, float* grad_sample, float* grad_probe,
                    void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- Fourier ptychography --------------------------------------------------------
+ * Operator  A[b] = |ifft2(fftshift(S[window_b] * pupil))|, S = fft2(object), window_b the
+ * (lh x lw) block at rows (ly+r+H/2) % H, columns (lx+c+W/2) % W of S.
+ * All four sides must be powers of two in [4, 1024].
+ * Replaces `_C.forward` / `_C.backward` of fpm_extension.cpp:21-60 and the torch path of
+ * python/ptychoX/fpm/ops.py:38-124.
+ */
+size_t ptx_fpm_workspace_bytes(int object_h, int object_w, int low_h, int low_w, int batch);
+
+/* Forward.  spectrum (OUT, complex64 [H, W]) = fft2(object), kept by the caller for the
+ * backward; image (complex64 [batch, lh, lw], may be NULL) and amplitude (float32).
+ * Replaces fpm_extension.cpp:21-32 (ptychox_fpm_forward_cuda, fpm_kernel.cu:233-273). */
+int ptx_fpm_forward(const float* object, int object_h, int object_w,
+                    const float* pupil, int low_h, int low_w,
+                    const int64_t* led_indices_xy, int batch,
+                    float* spectrum, float* image, float* amplitude,
+                    void* workspace, size_t workspace_bytes, void* stream);
+
+/* Adjoint for grad_output (float32 [batch, lh, lw]); image and spectrum as written by the
+ * forward.  grad_object (complex64 [H, W]) and grad_pupil are OVERWRITTEN.
+ * Replaces fpm_extension.cpp:34-60 (ptychox_fpm_backward_cuda, fpm_kernel.cu:275-317). */
+int ptx_fpm_backward(const float* grad_output, const float* image, const float* spectrum,
+                     int object_h, int object_w, const float* pupil, int low_h, int low_w,
+                     const int64_t* led_indices_xy, int batch,
+                     float* grad_object, float* grad_pupil,
+                     void* workspace, size_t workspace_bytes, void* stream);
+
+/* Fused sweep: mean((A - sqrt(scale * I))^2) in FP64 and its gradients (OVERWRITTEN),
+ * as F.mse_loss(ptychoX_fourier(...), observed).backward() (python/train_fpm.py:255-263). */
+int ptx_fpm_sweep(const float* object, int object_h, int object_w,
+                  const float* pupil, int low_h, int low_w,
+                  const int64_t* led_indices_xy, int batch,
+                  const uint16_t* measured, float scale,
+                  double* loss, float* grad_object, float* grad_pupil,
+                  void* workspace, size_t workspace_bytes, void* stream);
+
 /* Allocation-free fused sweep, for callers that cannot allocate device memory: a host
  * program that loads this library as a plug-in and keeps the GPU memory pool to itself,
  * or an acquisition loop that must not take the device-wide synchronisation of a

@@ -8,16 +8,23 @@ operator names, aliases and cache hooks, backed by ``libptychox`` (C ABI in
 from ._utils import matlab_positions_to_torch
 from .base import clear_cuda_plan_cache as clear_base_cuda_plan_cache
 from .base import ptychoX_base, ptychoX_base_loss, ptychography_base
+from .fpm import clear_cuda_plan_cache as clear_fpm_cuda_plan_cache
+from .fpm import fourier_ptychography, ptychoX_fourier, ptychoX_fourier_loss
 
 
 def clear_cuda_plan_cache() -> None:
     """Drop cached FFT plans of every modality (one shared library cache)."""
     clear_base_cuda_plan_cache()
+    clear_fpm_cuda_plan_cache()
 
 
 __all__ = [
     "clear_cuda_plan_cache",
     "clear_base_cuda_plan_cache",
+    "clear_fpm_cuda_plan_cache",
+    "ptychoX_fourier",
+    "ptychoX_fourier_loss",
+    "fourier_ptychography",
     "ptychoX_base",
     "ptychoX_base_loss",
     "ptychography_base",

@@ -1,0 +1,471 @@
+// Fourier ptychography (FPM): forward, adjoint and the fused forward+loss+adjoint sweep.
+//
+// Math (python/ptychoX/fpm/ops.py:180-183 forward, :209-221 adjoint, :113-124 windows):
+//   S = fft2(O);  sub_b[r,c] = S[(ly+r+H/2) % H, (lx+c+W/2) % W]
+//   image_b = ifft2(fftshift(sub_b * pupil)),  A_b = |image_b|
+//   Gl_b = ifftshift(fft2(g_b * image/max(|image|, eps)) / (h w))
+//   grad_pupil = sum_b Gl_b conj(sub_b);  grad_S[window_b] += Gl_b conj(pupil)
+//   grad_O = ifft2(grad_S) * H W
+//
+// Per frame (one LED) the same three-pass structure as the conventional sweep:
+//   row pass   gather the window of S (with wrap), x pupil, fftshift placement, inverse
+//              row DFT                                                         -> scratch
+//   col pass   inverse column DFT, image = X/(h w), |image|, residual vs sqrt(scale I),
+//              FP64 loss, g image/|image|, forward column DFT                  -> scratch
+//   row pass   forward row DFT, /(h w), ifftshift placement, grad_S += Gl conj(pupil)
+//              (float2 atomics, with wrap), grad_pupil += Gl conj(S) in registers
+// S = fft2(O) before the frames and grad_O = n ifft2(grad_S) after them use the generic
+// 2-D passes.  All sides are powers of two (4..1024), so every modulo is a mask.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "ptx_internal.h"
+#include "ptx_passes.cuh"
+
+namespace ptx {
+namespace {
+
+constexpr size_t kHdr = 256;
+enum FpmMode { kFpmSweep = 0, kFpmForward = 1, kFpmBackward = 2 };
+
+__device__ __forceinline__ int wrap2(long long v, int n) { return static_cast<int>(v & (long long)(n - 1)); }
+
+template <int NW>
+__global__ void __launch_bounds__(256, 2) fpm_rows_forward(
+    const float2* __restrict__ spec, int oh, int ow, const float2* __restrict__ pupil, int lh,
+    const int64_t* __restrict__ led, float2* __restrict__ scratch, const float2* __restrict__ tw, int lines) {
+  using S = RegShape<NW>;
+  constexpr int kTiles = (NW + kTile - 1) / kTile;
+  extern __shared__ float2 sm[];
+  const int tid = threadIdx.x;
+  const int l = tid / S::T;
+  const int t = tid - l * S::T;
+  const int i = blockIdx.x * lines + l;  // row of G = fftshift(sub * pupil)
+  const int f = blockIdx.y;
+  const bool row_ok = i < lh;
+  const long long lx = led[2 * f], ly = led[2 * f + 1];
+  const int r = (i + lh / 2) & (lh - 1);  // window row of that G row
+  const float2* srow = spec + (size_t)wrap2(ly + r + oh / 2, oh) * ow;
+  const float2* prow = pupil + (size_t)r * NW;
+  float2 v[S::N1];
+#pragma unroll
+  for (int j = 0; j < S::N1; ++j) {
+    const int c = (t + S::T * j + NW / 2) & (NW - 1);
+    v[j] = row_ok ? cmul(srow[wrap2(lx + c + ow / 2, ow)], __ldg(&prow[c])) : make_float2(0.f, 0.f);
+  }
+  reg_fft<NW, true, false>(v, sm + l * RowPass<NW>::LP, t, tw);
+  if (row_ok) {
+    float2* base = scratch + (size_t)f * kTiles * lh * kTile + (size_t)i * kTile;
+#pragma unroll
+    for (int m = 0; m < S::N1; ++m) {
+      const int kc = t + S::T * m;
+      base[(size_t)(kc / kTile) * lh * kTile + (kc % kTile)] = v[m];
+    }
+  }
+}
+
+template <int MODE, int NH>
+__global__ void __launch_bounds__(256, 2) fpm_cols(
+    float2* __restrict__ scratch, int lw, int frame0, const float2* __restrict__ tw,
+    const uint16_t* __restrict__ measured, float scale, float norm, float grad_scale, double inv_numel,
+    double* __restrict__ loss, float2* __restrict__ image_out, float* __restrict__ amplitude,
+    const float* __restrict__ grad_output) {
+  using S = RegShape<NH>;
+  using CP = ColPass<NH>;
+  extern __shared__ float2 sm[];
+  uint16_t* meas_s = reinterpret_cast<uint16_t*>(reinterpret_cast<char*>(sm) + CP::kMeasOffsetBytes);
+  const int tid = threadIdx.x;
+  const int c = tid % kColsPerCta;
+  const int t = tid / kColsPerCta;
+  constexpr int kSubs = kTile / kColsPerCta;
+  const int ct = blockIdx.x / kSubs;
+  const int c0 = ct * kTile + (blockIdx.x - ct * kSubs) * kColsPerCta;
+  const int f = blockIdx.y;
+  const int kc = c0 + c;
+  const bool col_ok = kc < lw;
+  const int tiles = num_tiles(lw);
+  float2* tile = scratch + ((size_t)f * tiles + ct) * NH * kTile + (c0 - ct * kTile);
+  const size_t g = (size_t)frame0 + f;
+  float2* buf = sm + c * CP::LP;
+  float2 v[S::N1];
+
+  if (MODE == kFpmSweep) {
+    const bool fast = (lw % (2 * kColsPerCta) == 0) && ((reinterpret_cast<uintptr_t>(measured) & 15) == 0);
+    if (fast) {
+      for (int kr = tid; kr < NH; kr += blockDim.x) cp_async16(meas_s + kr * kColsPerCta, measured + (g * NH + kr) * lw + c0);
+      cp_async_commit();
+    } else {
+      for (int q = tid; q < NH * kColsPerCta; q += blockDim.x) {
+        const int kr = q / kColsPerCta, cc = q - kr * kColsPerCta;
+        meas_s[q] = (c0 + cc < lw) ? measured[(g * NH + kr) * lw + c0 + cc] : 0;
+      }
+    }
+  }
+  if (MODE != kFpmBackward) {
+#pragma unroll
+    for (int j = 0; j < S::N1; ++j) v[j] = col_ok ? tile[(t + S::T * j) * kTile + c] : make_float2(0.f, 0.f);
+    reg_fft<NH, true, true>(v, buf, t, tw);
+  }
+  if (MODE == kFpmSweep) {
+    cp_async_wait_all();
+    __syncthreads();
+    double acc = 0.0;
+#pragma unroll
+    for (int m = 0; m < S::N1; ++m) {
+      const int kr = t + S::T * m;
+      const float2 im = cscale(v[m], norm);
+      float2 out = make_float2(0.f, 0.f);
+      if (col_ok) {
+        const float y = sqrtf(static_cast<float>(meas_s[kr * kColsPerCta + c]) * scale);
+        const float a = cabsf(im);
+        const float rr = a - y;
+        acc += static_cast<double>(rr) * static_cast<double>(rr);
+        out = cscale(im, grad_scale * rr / fmaxf(a, kEpsF32));
+      }
+      v[m] = out;
+    }
+    block_add_double(acc, inv_numel, loss);
+  } else if (MODE == kFpmForward) {
+    if (col_ok) {
+#pragma unroll
+      for (int m = 0; m < S::N1; ++m) {
+        const size_t idx = (g * NH + t + S::T * m) * lw + kc;
+        const float2 im = cscale(v[m], norm);
+        if (image_out) image_out[idx] = im;
+        amplitude[idx] = cabsf(im);
+      }
+    }
+    return;
+  } else {
+#pragma unroll
+    for (int m = 0; m < S::N1; ++m) {
+      float2 out = make_float2(0.f, 0.f);
+      if (col_ok) {
+        const size_t idx = (g * NH + t + S::T * m) * lw + kc;
+        const float2 im = image_out[idx];
+        out = cscale(im, grad_output[idx] / fmaxf(cabsf(im), kEpsF32));
+      }
+      v[m] = out;
+    }
+  }
+  reg_fft<NH, false, true>(v, buf, t, tw);
+  if (col_ok) {
+#pragma unroll
+    for (int m = 0; m < S::N1; ++m) tile[(t + S::T * m) * kTile + c] = v[m];
+  }
+}
+
+template <int NW>
+__global__ void __launch_bounds__(128, 3) fpm_rows_adjoint(
+    const float2* __restrict__ scratch, const float2* __restrict__ spec, int oh, int ow,
+    const float2* __restrict__ pupil, int lh, const int64_t* __restrict__ led, int nframes, int frames_per_cta,
+    float norm, float2* __restrict__ grad_spec, float2* __restrict__ grad_pupil, const float2* __restrict__ tw,
+    int lines) {
+  using S = RegShape<NW>;
+  constexpr int kTiles = (NW + kTile - 1) / kTile;
+  extern __shared__ float2 sm[];
+  const int tid = threadIdx.x;
+  const int l = tid / S::T;
+  const int t = tid - l * S::T;
+  const int i = blockIdx.x * lines + l;
+  const bool row_ok = i < lh;
+  const int r = (i + lh / 2) & (lh - 1);
+  const int f0 = blockIdx.y * frames_per_cta;
+  const int f1 = min(nframes, f0 + frames_per_cta);
+  float2* buf = sm + l * RowPass<NW>::LP;
+  float2* sbuf = sm + lines * RowPass<NW>::LP + l * NW;  // prefetched window row of S
+  const float2* prow = pupil + (size_t)r * NW;
+  float2 acc[S::N1];
+#pragma unroll
+  for (int m = 0; m < S::N1; ++m) acc[m] = make_float2(0.f, 0.f);
+  for (int f = f0; f < f1; ++f) {
+    const long long lx = led[2 * f], ly = led[2 * f + 1];
+    const size_t srow = (size_t)wrap2(ly + r + oh / 2, oh) * ow;
+    if (row_ok) {
+#pragma unroll
+      for (int m = 0; m < S::N1; ++m) {
+        const int jj = t + S::T * m;
+        const int c = (jj + NW / 2) & (NW - 1);
+        cp_async8(sbuf + jj, spec + srow + wrap2(lx + c + ow / 2, ow));
+      }
+      cp_async_commit();
+    }
+    float2 v[S::N1];
+    if (row_ok) {
+      const float2* base = scratch + (size_t)f * kTiles * lh * kTile + (size_t)i * kTile;
+#pragma unroll
+      for (int j = 0; j < S::N1; ++j) {
+        const int cc = t + S::T * j;
+        v[j] = base[(size_t)(cc / kTile) * lh * kTile + (cc % kTile)];
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < S::N1; ++j) v[j] = make_float2(0.f, 0.f);
+    }
+    reg_fft<NW, false, false>(v, buf, t, tw);
+    if (row_ok) {
+      cp_async_wait_all();
+#pragma unroll
+      for (int m = 0; m < S::N1; ++m) {
+        const int jj = t + S::T * m;
+        const int c = (jj + NW / 2) & (NW - 1);
+        const float2 gl = cscale(v[m], norm);
+        atomicAdd(&grad_spec[srow + wrap2(lx + c + ow / 2, ow)], cmulc(gl, __ldg(&prow[c])));
+        acc[m] = cadd(acc[m], cmulc(gl, sbuf[jj]));
+      }
+    }
+  }
+  if (row_ok) {
+#pragma unroll
+    for (int m = 0; m < S::N1; ++m) {
+      const int c = (t + S::T * m + NW / 2) & (NW - 1);
+      atomicAdd(&grad_pupil[(size_t)r * NW + c], acc[m]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------------------
+
+struct FpmGeom {
+  int oh, ow, lh, lw, batch;
+  LinePlan p_ow, p_oh, p_lw, p_lh;
+  size_t spec_bytes, tmp_bytes, frame_bytes;
+  int chunk;
+  float2* spec;   // workspace spectrum (sweep)
+  float2* gspec;  // gradient w.r.t. the spectrum
+  float2* tmp;    // tiled temporary of the 2-D passes
+  float2* frames;
+};
+
+size_t fpm_fixed_bytes(int oh, int ow) {
+  const size_t spec = (size_t)oh * ow * sizeof(float2);
+  const size_t tmp = (size_t)num_tiles(ow) * kTile * oh * sizeof(float2);
+  return kHdr + 2 * spec + tmp;
+}
+
+int fpm_check(const void* object, int oh, int ow, const void* pupil, int lh, int lw, const int64_t* led, int batch,
+              void* ws, size_t ws_bytes, FpmGeom* g) {
+  if (!object || !pupil || (!led && batch > 0) || !ws) return set_error(PTX_ERR_INVALID_ARGUMENT, "null pointer argument");
+  if (batch < 0) return set_error(PTX_ERR_INVALID_ARGUMENT, "negative batch");
+  for (int n : {oh, ow, lh, lw}) {
+    if (!is_pow2_len(n)) {
+      return set_error(PTX_ERR_UNSUPPORTED_SIZE, "FPM sides must be powers of two in [4, 1024] (got %d)", n);
+    }
+  }
+  if (lh > oh || lw > ow) return set_error(PTX_ERR_INVALID_ARGUMENT, "pupil larger than the object spectrum");
+  g->oh = oh; g->ow = ow; g->lh = lh; g->lw = lw; g->batch = batch;
+  if (int st = get_line_plan(ow, &g->p_ow)) return st;
+  if (int st = get_line_plan(oh, &g->p_oh)) return st;
+  if (int st = get_line_plan(lw, &g->p_lw)) return st;
+  if (int st = get_line_plan(lh, &g->p_lh)) return st;
+  g->spec_bytes = (size_t)oh * ow * sizeof(float2);
+  g->tmp_bytes = (size_t)num_tiles(ow) * kTile * oh * sizeof(float2);
+  g->frame_bytes = (size_t)num_tiles(lw) * kTile * lh * sizeof(float2);
+  const size_t fixed = fpm_fixed_bytes(oh, ow);
+  if (ws_bytes < fixed + g->frame_bytes) {
+    return set_error(PTX_ERR_WORKSPACE, "workspace of %zu bytes is smaller than the %zu bytes needed", ws_bytes,
+                     fixed + g->frame_bytes);
+  }
+  g->chunk = static_cast<int>(std::min<size_t>((ws_bytes - fixed) / g->frame_bytes, (size_t)std::max(batch, 1)));
+  char* p = static_cast<char*>(ws) + kHdr;
+  g->spec = reinterpret_cast<float2*>(p);
+  g->gspec = reinterpret_cast<float2*>(p + g->spec_bytes);
+  g->tmp = reinterpret_cast<float2*>(p + 2 * g->spec_bytes);
+  g->frames = reinterpret_cast<float2*>(p + 2 * g->spec_bytes + g->tmp_bytes);
+  int st = PTX_OK;
+  dispatch_pow2(ow, [&](auto NT) {
+    constexpr int N = decltype(NT)::value;
+    if (!st) st = ensure_smem((const void*)fft2_rows_kernel<N, false>, RowPass<N>::smem(RowPass<N>::lines(256, oh)));
+    if (!st) st = ensure_smem((const void*)fft2_rows_kernel<N, true>, RowPass<N>::smem(RowPass<N>::lines(256, oh)));
+  });
+  dispatch_pow2(oh, [&](auto NT) {
+    constexpr int N = decltype(NT)::value;
+    const int sm = kColsPerCta * ColPass<N>::LP * (int)sizeof(float2);
+    if (!st) st = ensure_smem((const void*)fft2_cols_kernel<N, false>, sm);
+    if (!st) st = ensure_smem((const void*)fft2_cols_kernel<N, true>, sm);
+  });
+  dispatch_pow2(lw, [&](auto NT) {
+    constexpr int N = decltype(NT)::value;
+    if (!st) st = ensure_smem((const void*)fpm_rows_forward<N>, RowPass<N>::smem(RowPass<N>::lines(256, lh)));
+    if (!st) st = ensure_smem((const void*)fpm_rows_adjoint<N>, RowPass<N>::smem_with_row(RowPass<N>::lines(128, lh)));
+  });
+  dispatch_pow2(lh, [&](auto NT) {
+    constexpr int N = decltype(NT)::value;
+    if (!st) st = ensure_smem((const void*)fpm_cols<kFpmSweep, N>, ColPass<N>::kSmemBytes);
+    if (!st) st = ensure_smem((const void*)fpm_cols<kFpmForward, N>, ColPass<N>::kSmemBytes);
+    if (!st) st = ensure_smem((const void*)fpm_cols<kFpmBackward, N>, ColPass<N>::kSmemBytes);
+  });
+  return st;
+}
+
+// out = DFT2 (INV=false) or unnormalised inverse DFT2 (INV=true) of in, via tmp.
+template <bool INV>
+void launch_fft2(const float2* in, int H, int W, float2* out, float scale, float2* tmp, const LinePlan& prow,
+                 const LinePlan& pcol, cudaStream_t s) {
+  prof_begin(kFft2Rows, s);
+  dispatch_pow2(W, [&](auto NT) {
+    constexpr int N = decltype(NT)::value;
+    const int lines = RowPass<N>::lines(256, H);
+    fft2_rows_kernel<N, INV><<<(H + lines - 1) / lines, lines * RowPass<N>::T, RowPass<N>::smem(lines), s>>>(
+        in, H, tmp, prow.tw, lines);
+  });
+  prof_end(kFft2Rows, s);
+  prof_begin(kFft2Cols, s);
+  dispatch_pow2(H, [&](auto NT) {
+    constexpr int N = decltype(NT)::value;
+    const int sm = kColsPerCta * ColPass<N>::LP * (int)sizeof(float2);
+    fft2_cols_kernel<N, INV><<<num_tiles(W) * (kTile / kColsPerCta), ColPass<N>::kThreads, sm, s>>>(
+        tmp, W, out, scale, pcol.tw);
+  });
+  prof_end(kFft2Cols, s);
+}
+
+void launch_rows_forward(const FpmGeom& g, const float2* spec, const float2* pupil, const int64_t* led, int nf,
+                         cudaStream_t s) {
+  prof_begin(kFpmRowsForward, s);
+  dispatch_pow2(g.lw, [&](auto NT) {
+    constexpr int N = decltype(NT)::value;
+    const int lines = RowPass<N>::lines(256, g.lh);
+    dim3 grid((g.lh + lines - 1) / lines, nf);
+    fpm_rows_forward<N><<<grid, lines * RowPass<N>::T, RowPass<N>::smem(lines), s>>>(
+        spec, g.oh, g.ow, pupil, g.lh, led, g.frames, g.p_lw.tw, lines);
+  });
+  prof_end(kFpmRowsForward, s);
+}
+
+template <int MODE>
+void launch_cols(const FpmGeom& g, int frame0, int nf, const uint16_t* measured, float scale, float grad_scale,
+                 double inv_numel, double* loss, float2* image, float* amplitude, const float* grad_output,
+                 cudaStream_t s) {
+  const float norm = 1.0f / static_cast<float>((double)g.lh * g.lw);
+  prof_begin(kFpmCols, s);
+  dispatch_pow2(g.lh, [&](auto NT) {
+    constexpr int N = decltype(NT)::value;
+    dim3 grid(num_tiles(g.lw) * (kTile / kColsPerCta), nf);
+    fpm_cols<MODE, N><<<grid, ColPass<N>::kThreads, ColPass<N>::kSmemBytes, s>>>(
+        g.frames, g.lw, frame0, g.p_lh.tw, measured, scale, norm, grad_scale, inv_numel, loss, image, amplitude,
+        grad_output);
+  });
+  prof_end(kFpmCols, s);
+}
+
+void launch_rows_adjoint(const FpmGeom& g, const float2* spec, const float2* pupil, const int64_t* led, int nf,
+                         float2* grad_spec, float2* grad_pupil, cudaStream_t s) {
+  const float norm = 1.0f / static_cast<float>((double)g.lh * g.lw);
+  prof_begin(kFpmRowsAdjoint, s);
+  dispatch_pow2(g.lw, [&](auto NT) {
+    constexpr int N = decltype(NT)::value;
+    const int lines = RowPass<N>::lines(128, g.lh);
+    const int rowgroups = (g.lh + lines - 1) / lines;
+    const long long ctas_one = (long long)rowgroups * nf;
+    const int fpc = std::max(1, std::min<int>(nf, static_cast<int>(ctas_one / (sm_count() * 6))));
+    dim3 grid(rowgroups, (nf + fpc - 1) / fpc);
+    fpm_rows_adjoint<N><<<grid, lines * RowPass<N>::T, RowPass<N>::smem_with_row(lines), s>>>(
+        g.frames, spec, g.oh, g.ow, pupil, g.lh, led, nf, fpc, norm, grad_spec, grad_pupil, g.p_lw.tw, lines);
+  });
+  prof_end(kFpmRowsAdjoint, s);
+}
+
+}  // namespace
+}  // namespace ptx
+
+using namespace ptx;
+
+extern "C" {
+
+size_t ptx_fpm_workspace_bytes(int object_h, int object_w, int low_h, int low_w, int batch) {
+  if (object_h <= 0 || object_w <= 0 || low_h <= 0 || low_w <= 0) return 0;
+  const size_t frame = (size_t)num_tiles(low_w) * kTile * low_h * sizeof(float2);
+  const size_t frames = std::max<size_t>(1, std::min<size_t>((size_t)std::max(batch, 1), (4096ull << 20) / frame));
+  return fpm_fixed_bytes(object_h, object_w) + frames * frame;
+}
+
+int ptx_fpm_forward(const float* object, int object_h, int object_w, const float* pupil, int low_h, int low_w,
+                    const int64_t* led_indices_xy, int batch, float* spectrum, float* image, float* amplitude,
+                    void* workspace, size_t workspace_bytes, void* stream) {
+  FpmGeom g;
+  if (int st = fpm_check(object, object_h, object_w, pupil, low_h, low_w, led_indices_xy, batch, workspace,
+                         workspace_bytes, &g)) {
+    return st;
+  }
+  if (!spectrum || (!amplitude && batch > 0)) return set_error(PTX_ERR_INVALID_ARGUMENT, "null output");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  float2* spec = reinterpret_cast<float2*>(spectrum);
+  launch_fft2<false>(reinterpret_cast<const float2*>(object), object_h, object_w, spec, 1.0f, g.tmp, g.p_ow, g.p_oh, s);
+  const float2* P = reinterpret_cast<const float2*>(pupil);
+  for (int b0 = 0; b0 < batch; b0 += g.chunk) {
+    const int nf = std::min(g.chunk, batch - b0);
+    launch_rows_forward(g, spec, P, led_indices_xy + 2 * (size_t)b0, nf, s);
+    launch_cols<kFpmForward>(g, b0, nf, nullptr, 0.f, 0.f, 0.0, nullptr, reinterpret_cast<float2*>(image),
+                             amplitude, nullptr, s);
+  }
+  return cuda_status(cudaGetLastError(), "ptx_fpm_forward launch");
+}
+
+int ptx_fpm_backward(const float* grad_output, const float* image, const float* spectrum, int object_h,
+                     int object_w, const float* pupil, int low_h, int low_w, const int64_t* led_indices_xy, int batch,
+                     float* grad_object, float* grad_pupil, void* workspace, size_t workspace_bytes, void* stream) {
+  FpmGeom g;
+  if (int st = fpm_check(spectrum, object_h, object_w, pupil, low_h, low_w, led_indices_xy, batch, workspace,
+                         workspace_bytes, &g)) {
+    return st;
+  }
+  if (((!grad_output || !image) && batch > 0) || !grad_object || !grad_pupil) {
+    return set_error(PTX_ERR_INVALID_ARGUMENT, "null pointer argument");
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaMemsetAsync(g.gspec, 0, g.spec_bytes, s);
+  cudaMemsetAsync(grad_pupil, 0, sizeof(float2) * (size_t)low_h * low_w, s);
+  const float2* spec = reinterpret_cast<const float2*>(spectrum);
+  const float2* P = reinterpret_cast<const float2*>(pupil);
+  float2* GP = reinterpret_cast<float2*>(grad_pupil);
+  for (int b0 = 0; b0 < batch; b0 += g.chunk) {
+    const int nf = std::min(g.chunk, batch - b0);
+    launch_cols<kFpmBackward>(g, b0, nf, nullptr, 0.f, 0.f, 0.0, nullptr,
+                              const_cast<float2*>(reinterpret_cast<const float2*>(image)), nullptr, grad_output, s);
+    launch_rows_adjoint(g, spec, P, led_indices_xy + 2 * (size_t)b0, nf, g.gspec, GP, s);
+  }
+  launch_fft2<true>(g.gspec, object_h, object_w, reinterpret_cast<float2*>(grad_object), 1.0f, g.tmp, g.p_ow, g.p_oh,
+                    s);
+  return cuda_status(cudaGetLastError(), "ptx_fpm_backward launch");
+}
+
+int ptx_fpm_sweep(const float* object, int object_h, int object_w, const float* pupil, int low_h, int low_w,
+                  const int64_t* led_indices_xy, int batch, const uint16_t* measured, float scale, double* loss,
+                  float* grad_object, float* grad_pupil, void* workspace, size_t workspace_bytes, void* stream) {
+  FpmGeom g;
+  if (int st = fpm_check(object, object_h, object_w, pupil, low_h, low_w, led_indices_xy, batch, workspace,
+                         workspace_bytes, &g)) {
+    return st;
+  }
+  if ((!measured && batch > 0) || !loss || !grad_object || !grad_pupil) {
+    return set_error(PTX_ERR_INVALID_ARGUMENT, "null pointer argument");
+  }
+  if (!(scale > 0.f)) return set_error(PTX_ERR_INVALID_ARGUMENT, "scale must be positive");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaMemsetAsync(g.gspec, 0, g.spec_bytes, s);
+  cudaMemsetAsync(grad_pupil, 0, sizeof(float2) * (size_t)low_h * low_w, s);
+  cudaMemsetAsync(loss, 0, sizeof(double), s);
+  const double numel = (double)batch * low_h * low_w;
+  const float grad_scale = static_cast<float>(2.0 / std::max(numel, 1.0));
+  launch_fft2<false>(reinterpret_cast<const float2*>(object), object_h, object_w, g.spec, 1.0f, g.tmp, g.p_ow, g.p_oh,
+                     s);
+  const float2* P = reinterpret_cast<const float2*>(pupil);
+  float2* GP = reinterpret_cast<float2*>(grad_pupil);
+  for (int b0 = 0; b0 < batch; b0 += g.chunk) {
+    const int nf = std::min(g.chunk, batch - b0);
+    const int64_t* led = led_indices_xy + 2 * (size_t)b0;
+    launch_rows_forward(g, g.spec, P, led, nf, s);
+    launch_cols<kFpmSweep>(g, b0, nf, measured, scale, grad_scale, 1.0 / std::max(numel, 1.0), loss, nullptr, nullptr,
+                           nullptr, s);
+    launch_rows_adjoint(g, g.spec, P, led, nf, g.gspec, GP, s);
+  }
+  launch_fft2<true>(g.gspec, object_h, object_w, reinterpret_cast<float2*>(grad_object), 1.0f, g.tmp, g.p_ow, g.p_oh,
+                    s);
+  return cuda_status(cudaGetLastError(), "ptx_fpm_sweep launch");
+}
+
+}  // extern "C"

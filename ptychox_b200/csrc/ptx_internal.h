@@ -65,6 +65,25 @@ enum KernelId {
 void prof_begin(int id, cudaStream_t s);
 void prof_end(int id, cudaStream_t s);
 
+// Power-of-two line lengths 4..1024 (the register-FFT kernels); returns false (and calls
+// nothing) for any other length.
+template <typename F>
+bool dispatch_pow2(int n, F&& f) {
+  switch (n) {
+    case 4: f(std::integral_constant<int, 4>{}); return true;
+    case 8: f(std::integral_constant<int, 8>{}); return true;
+    case 16: f(std::integral_constant<int, 16>{}); return true;
+    case 32: f(std::integral_constant<int, 32>{}); return true;
+    case 64: f(std::integral_constant<int, 64>{}); return true;
+    case 128: f(std::integral_constant<int, 128>{}); return true;
+    case 256: f(std::integral_constant<int, 256>{}); return true;
+    case 512: f(std::integral_constant<int, 512>{}); return true;
+    case 1024: f(std::integral_constant<int, 1024>{}); return true;
+    default: return false;
+  }
+}
+inline bool is_pow2_len(int n) { return n >= 4 && n <= 1024 && (n & (n - 1)) == 0; }
+
 // Line lengths that get compile-time FFT plans; every other supported length runs the
 // runtime-plan kernels (template argument 0).
 template <typename F>

@@ -1,0 +1,124 @@
+// Pieces shared by the modality kernels built on the register FFT: launch shapes, the
+// FP64 block reduction of loss partials, and generic 2-D transform passes between a
+// natural row-major array and the tiled frame layout [tile][row][16].
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "ptx_regfft.cuh"
+
+namespace ptx {
+
+constexpr float kEpsF32 = 1.1920928955078125e-07f;  // torch.finfo(float32).eps
+constexpr int kColsPerCta = 8;                        // columns per column-pass CTA
+
+template <int N>
+struct RowPass {
+  static constexpr int T = RegShape<N>::T;
+  static constexpr int LP = row_line_pitch<N>();
+  // rows per CTA (a whole number of warps)
+  __host__ static int lines(int threads, int rows) {
+    int l = threads / T;
+    if (l < 1) l = 1;
+    const int quantum = T >= 32 ? 1 : 32 / T;
+    const int need = ((rows + quantum - 1) / quantum) * quantum;
+    return l < need ? l : need;
+  }
+  __host__ static int smem(int lines) { return lines * LP * (int)sizeof(float2); }
+  // exchange buffers plus one prefetched row of N complex values per line
+  __host__ static int smem_with_row(int lines) { return lines * (LP + N) * (int)sizeof(float2); }
+};
+
+template <int N>
+struct ColPass {
+  static constexpr int T = RegShape<N>::T;
+  static constexpr int LP = col_line_pitch<N>();
+  static constexpr int kThreads = kColsPerCta * T;
+  static constexpr int kMeasOffsetBytes = ((kColsPerCta * LP * (int)sizeof(float2)) + 15) / 16 * 16;
+  static constexpr int kSmemBytes = kMeasOffsetBytes + N * kColsPerCta * (int)sizeof(uint16_t);
+};
+
+// Sum a per-thread FP64 partial over the block and add it (times `scale`) to *out.
+// Every thread of the block must call it; blocks smaller than a warp take the
+// shared-memory atomic route (a full-mask shuffle needs all 32 lanes).
+__device__ __forceinline__ void block_add_double(double v, double scale, double* out) {
+  __shared__ double red[32];
+  const int tid = threadIdx.x;
+  if ((blockDim.x & 31) == 0) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((tid & 31) == 0) red[tid >> 5] = v;
+    __syncthreads();
+    if (tid < 32) {
+      const int nw = blockDim.x >> 5;
+      double w = (tid < nw) ? red[tid] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+      if (tid == 0) atomicAdd(out, w * scale);
+    }
+  } else {
+    if (tid == 0) red[0] = 0.0;
+    __syncthreads();
+    atomicAdd(&red[0], v);
+    __syncthreads();
+    if (tid == 0) atomicAdd(out, red[0] * scale);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Generic 2-D transform passes (unnormalised; INV selects the sign)
+// ---------------------------------------------------------------------------------------
+
+// Row pass: in [H][N] natural -> row DFT -> tiled [N/16][H][16].
+template <int N, bool INV>
+__global__ void __launch_bounds__(256, 2) fft2_rows_kernel(const float2* __restrict__ in, int H,
+                                                            float2* __restrict__ tiled,
+                                                            const float2* __restrict__ tw, int lines) {
+  using S = RegShape<N>;
+  extern __shared__ float2 sm[];
+  const int tid = threadIdx.x;
+  const int l = tid / S::T;
+  const int t = tid - l * S::T;
+  const int r = blockIdx.x * lines + l;
+  const bool row_ok = r < H;
+  float2 v[S::N1];
+#pragma unroll
+  for (int j = 0; j < S::N1; ++j) v[j] = row_ok ? in[(size_t)r * N + t + S::T * j] : make_float2(0.f, 0.f);
+  reg_fft<N, INV, false>(v, sm + l * RowPass<N>::LP, t, tw);
+  if (row_ok) {
+#pragma unroll
+    for (int m = 0; m < S::N1; ++m) {
+      const int kc = t + S::T * m;
+      tiled[((size_t)(kc / kTile) * H + r) * kTile + (kc % kTile)] = v[m];
+    }
+  }
+}
+
+// Column pass: tiled [tiles][N][16] -> column DFT -> out [N][W] natural, times `scale`.
+template <int N, bool INV>
+__global__ void __launch_bounds__(256, 2) fft2_cols_kernel(const float2* __restrict__ tiled, int W,
+                                                            float2* __restrict__ out, float scale,
+                                                            const float2* __restrict__ tw) {
+  using S = RegShape<N>;
+  extern __shared__ float2 sm[];
+  const int tid = threadIdx.x;
+  const int c = tid % kColsPerCta;
+  const int t = tid / kColsPerCta;
+  constexpr int kSubs = kTile / kColsPerCta;
+  const int ct = blockIdx.x / kSubs;
+  const int c0 = ct * kTile + (blockIdx.x - ct * kSubs) * kColsPerCta;
+  const int kc = c0 + c;
+  const bool col_ok = kc < W;
+  const float2* tile = tiled + (size_t)ct * N * kTile + (c0 - ct * kTile);
+  float2 v[S::N1];
+#pragma unroll
+  for (int j = 0; j < S::N1; ++j) v[j] = col_ok ? tile[(t + S::T * j) * kTile + c] : make_float2(0.f, 0.f);
+  reg_fft<N, INV, true>(v, sm + c * ColPass<N>::LP, t, tw);
+  if (col_ok) {
+#pragma unroll
+    for (int m = 0; m < S::N1; ++m) out[(size_t)(t + S::T * m) * W + kc] = cscale(v[m], scale);
+  }
+}
+
+}  // namespace ptx

@@ -1,4 +1,4 @@
-// Register-resident two-step FFT for compile-time power-of-two lengths 16..1024.
+// Register-resident two-step FFT for compile-time power-of-two lengths 4..1024.
 //
 // A line of length N = N1 * T is held by T threads, thread t owning the N1 values
 // x[t + T j] (j < N1) -- consecutive threads own consecutive elements, so a line is
@@ -28,7 +28,7 @@ struct RegShape {
   static constexpr int C = N1 / T;                 // step-3 DFTs per thread (1 or 2)
   static constexpr int RP = T + 1;                 // exchange row pitch (odd)
   static constexpr int BUF = N1 * RP;              // exchange buffer per line (float2)
-  static_assert((1 << LOG) == N && N >= 16 && N <= 1024, "power of two in [16, 1024]");
+  static_assert((1 << LOG) == N && N >= 4 && N <= 1024, "power of two in [4, 1024]");
 };
 
 // cos(2 pi m / 32) and sin(2 pi m / 32), m in [0, 32): after unrolling, m is a compile-time

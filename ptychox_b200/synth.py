@@ -80,16 +80,18 @@ def raster_positions(grid: int, step: int, origin: int, jitter: int,
 
 
 def poisson_counts(model_intensity: np.ndarray, photons: float, rng: np.random.Generator | None = None,
-                   per_pixel: bool = False) -> tuple[np.ndarray, float]:
+                   per_pixel: bool = False, brightest: bool = False) -> tuple[np.ndarray, float]:
     """Poisson uint16 counts of ``I / scale`` and the ``scale`` that decodes them.
 
-    ``scale`` makes an average pattern hold ``photons`` counts in total (or, with
-    ``per_pixel``, an average pixel hold ``photons`` counts).  The decoded amplitude is
-    ``sqrt(scale * counts)``.  Raises if any count exceeds uint16.
+    ``scale`` makes an average pattern (or, with ``brightest``, the brightest pattern) hold
+    ``photons`` counts in total — with ``per_pixel``, ``photons`` counts per pixel on
+    average.  The decoded amplitude is ``sqrt(scale * counts)``.  Raises if any count
+    exceeds uint16.
     """
     rng = rng or np.random.default_rng(0)
     inten = np.asarray(model_intensity, dtype=np.float64)
-    per_pattern = inten.reshape(inten.shape[0], -1).sum(axis=1).mean()
+    sums = inten.reshape(inten.shape[0], -1).sum(axis=1)
+    per_pattern = sums.max() if brightest else sums.mean()
     denom = photons if not per_pixel else photons * inten[0].size
     scale = float(per_pattern / denom)
     counts = rng.poisson(inten / scale)
