@@ -151,6 +151,47 @@ int ptx_fpm_sweep(const float* object, int object_h, int object_w,
                   double* loss, float* grad_object, float* grad_pupil,
                   void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- coded and near-field ptychography ------------------------------------------
+ * Operator  x_b = ifft2(fft2(O) T1 R_b),  s_b = ifft2(fft2(x_b M) T2),
+ * A_b = sqrt(avgpool_ds |s_b|^2),  R_b = exp(2 pi i (dx_b fx + dy_b fy)) with signed
+ * integer frequencies and shifts_xy float32 [batch, 2] (dx, dy) in units of the field side.
+ * transfer_1 = NULL gives near-field ptychography (T1 = 1).  Square fields, n a power of
+ * two in [16, 1024]; downsample must divide n (and 8).
+ * Replaces `_C.forward` / `_C.backward` of coded_extension.cpp:26-88 and the torch path
+ * of python/ptychoX/coded/ops.py:22-171; near-field replaces the MATLAB operator
+ * adPtychoX_nearf (fwd_adPtychoX_nearf.cu, bwd_adPtychoX_nearf.cu) with the exact
+ * RMS-pool gradient.
+ */
+size_t ptx_coded_workspace_bytes(int n, int batch);
+
+/* Forward: x_forward, sensor (complex64 [batch, n, n], saved for the backward) and
+ * amplitude (float32 [batch, n/ds, n/ds]).  Replaces coded_kernel.cu:283-345. */
+int ptx_coded_forward(const float* object, const float* coded_surface,
+                      const float* transfer_1, const float* transfer_2, int n,
+                      const float* shifts_xy, int batch, int downsample,
+                      float* x_forward, float* sensor, float* amplitude,
+                      void* workspace, size_t workspace_bytes, void* stream);
+
+/* Adjoint for grad_output (float32 [batch, n/ds, n/ds]) from the saved forward arrays;
+ * grad_object and grad_coded (complex64 [n, n]) are OVERWRITTEN.
+ * Replaces coded_kernel.cu:347-424. */
+int ptx_coded_backward(const float* grad_output, const float* x_forward, const float* sensor,
+                       const float* amplitude, const float* coded_surface,
+                       const float* transfer_1, const float* transfer_2, int n,
+                       const float* shifts_xy, int batch, int downsample,
+                       float* grad_object, float* grad_coded,
+                       void* workspace, size_t workspace_bytes, void* stream);
+
+/* Fused sweep: mean((A - sqrt(scale * I))^2) in FP64 (I uint16 [batch, n/ds, n/ds]) and
+ * its gradients (OVERWRITTEN), as F.mse_loss(ptychoX_coded(...), observed).backward()
+ * (python/train_coded.py:225-237). */
+int ptx_coded_sweep(const float* object, const float* coded_surface,
+                    const float* transfer_1, const float* transfer_2, int n,
+                    const float* shifts_xy, int batch, int downsample,
+                    const uint16_t* measured, float scale,
+                    double* loss, float* grad_object, float* grad_coded,
+                    void* workspace, size_t workspace_bytes, void* stream);
+
 /* Allocation-free fused sweep, for callers that cannot allocate device memory: a host
  * program that loads this library as a plug-in and keeps the GPU memory pool to itself,
  * or an acquisition loop that must not take the device-wide synchronisation of a

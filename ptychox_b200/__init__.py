@@ -8,6 +8,15 @@ operator names, aliases and cache hooks, backed by ``libptychox`` (C ABI in
 from ._utils import matlab_positions_to_torch
 from .base import clear_cuda_plan_cache as clear_base_cuda_plan_cache
 from .base import ptychoX_base, ptychoX_base_loss, ptychography_base
+from .coded import clear_cuda_plan_cache as clear_coded_cuda_plan_cache
+from .coded import (
+    coded_ptychography,
+    nearfield_ptychography,
+    ptychoX_coded,
+    ptychoX_coded_loss,
+    ptychoX_nearfield,
+    ptychoX_nearfield_loss,
+)
 from .fpm import clear_cuda_plan_cache as clear_fpm_cuda_plan_cache
 from .fpm import fourier_ptychography, ptychoX_fourier, ptychoX_fourier_loss
 
@@ -16,12 +25,20 @@ def clear_cuda_plan_cache() -> None:
     """Drop cached FFT plans of every modality (one shared library cache)."""
     clear_base_cuda_plan_cache()
     clear_fpm_cuda_plan_cache()
+    clear_coded_cuda_plan_cache()
 
 
 __all__ = [
     "clear_cuda_plan_cache",
     "clear_base_cuda_plan_cache",
     "clear_fpm_cuda_plan_cache",
+    "clear_coded_cuda_plan_cache",
+    "ptychoX_coded",
+    "ptychoX_coded_loss",
+    "coded_ptychography",
+    "ptychoX_nearfield",
+    "ptychoX_nearfield_loss",
+    "nearfield_ptychography",
     "ptychoX_fourier",
     "ptychoX_fourier_loss",
     "fourier_ptychography",

@@ -46,6 +46,10 @@ SIGNATURES: dict[str, tuple] = {
     "ptx_fpm_forward": (_i, [_p, _i, _i, _p, _i, _i, _p, _i, _p, _p, _p, _p, _sz, _p]),
     "ptx_fpm_backward": (_i, [_p, _p, _p, _i, _i, _p, _i, _i, _p, _i, _p, _p, _p, _sz, _p]),
     "ptx_fpm_sweep": (_i, [_p, _i, _i, _p, _i, _i, _p, _i, _p, _f, _p, _p, _p, _p, _sz, _p]),
+    "ptx_coded_workspace_bytes": (_sz, [_i, _i]),
+    "ptx_coded_forward": (_i, [_p, _p, _p, _p, _i, _p, _i, _i, _p, _p, _p, _p, _sz, _p]),
+    "ptx_coded_backward": (_i, [_p, _p, _p, _p, _p, _p, _p, _i, _p, _i, _i, _p, _p, _p, _sz, _p]),
+    "ptx_coded_sweep": (_i, [_p, _p, _p, _p, _i, _p, _i, _i, _p, _f, _p, _p, _p, _p, _sz, _p]),
     "ptx_base_sweep_noalloc": (_i, [_p, _i, _i, _p, _i, _i, _p, _i, _p, _f, _p, _p, _p, _p]),
 }
 

@@ -1,0 +1,584 @@
+// Coded and near-field ptychography: forward, adjoint and the fused sweep.
+//
+// Math (python/ptychoX/coded/ops.py:136-171; near-field = transfer_1 = 1, the MATLAB
+// sequence fwd_adPtychoX_nearf.cu:58-114 without the first transfer function):
+//   O^ = fft2(O);  x_b = ifft2(O^ T1 R_b)     R_b = exp(2 pi i (dx_b fx + dy_b fy))
+//   s_b = ifft2(fft2(x_b M) T2);  A_b = sqrt(avgpool_ds |s_b|^2)
+// Adjoint (the vector-Jacobian product autograd takes through that forward; step order as
+// in coded_kernel.cu:347-424):
+//   g_s = g / (A ds^2) s;  g_a = ifft2(fft2(g_s) conj(T2));  grad_M += g_a conj(x)
+//   g_X = fft2(g_a conj(M)) / n;  grad_O^ += g_X conj(T1 R_b);  grad_O = n ifft2(grad_O^)
+//
+// With unnormalised transforms D (forward) and D* (inverse), every 2-D transform is a
+// row pass and a column pass, and consecutive 1-D transforms along the same axis with a
+// pointwise step between them share one pass.  Seven passes per frame:
+//   1 col: load O^ T1 R_b, inverse column DFT                                  -> frame
+//   2 row: inverse row DFT, x = ./n (stored), a = x M, forward row DFT          -> frame
+//   3 col: forward column DFT, x T2, inverse column DFT                         -> frame
+//   4 row: inverse row DFT, s = ./n, RMS pool, FP64 loss, g_s, forward row DFT  -> frame
+//   5 col: forward column DFT, x conj(T2)/n, inverse column DFT                 -> frame
+//   6 row: inverse row DFT (g_a), grad_M += g_a conj(x) in registers,
+//          g_a conj(M), forward row DFT                                         -> frame
+//   7 col: forward column DFT, /n, grad_O^ += . conj(T1 R_b) (float2 atomics)
+// O^ = D(O) before the frames and grad_O = D*(grad_O^) after them use the generic 2-D
+// passes.  The phase ramp's argument is reduced exactly in FP32 (FMA two-product and
+// integer rounding) before sincospif, so the ramp is accurate to ~1 ulp of a turn.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "ptx_internal.h"
+#include "ptx_passes.cuh"
+
+namespace ptx {
+namespace {
+
+constexpr size_t kHdr = 256;
+enum CodedMode { kCodedSweep = 0, kCodedForward = 1, kCodedBackward = 2 };
+constexpr float kAmpFloor = 1e-30f;  // keeps g / A finite when a pooled amplitude is exactly 0
+
+// exp(2 pi i (dx fx + dy fy)) for signed integer frequencies fx, fy.
+__device__ __forceinline__ float2 shift_ramp(float dx, float dy, int fx, int fy) {
+  const float ffx = static_cast<float>(fx), ffy = static_cast<float>(fy);
+  const float px = dx * ffx, py = dy * ffy;
+  const float ex = fmaf(dx, ffx, -px), ey = fmaf(dy, ffy, -py);  // exact product remainders
+  const float t = (px - rintf(px)) + (py - rintf(py)) + (ex + ey);  // turns, |t| < ~1
+  float s, c;
+  sincospif(2.0f * t, &s, &c);
+  return make_float2(c, s);
+}
+
+__device__ __forceinline__ int signed_freq(int k, int n) { return k < n / 2 ? k : k - n; }
+
+// ---- column passes ---------------------------------------------------------------------
+// STAGE 1: load O^ T1 R, inverse DFT.  STAGE 3: forward DFT, x T2 (or conj(T2)/n when
+// CONJ), inverse DFT.  STAGE 7: forward DFT, /n, grad_O^ += . conj(T1 R).
+template <int STAGE, bool CONJ, int N>
+__global__ void __launch_bounds__(256, 2) coded_cols(
+    float2* __restrict__ scratch, const float2* __restrict__ ospec, const float2* __restrict__ t1,
+    const float2* __restrict__ t2, const float* __restrict__ shifts, float inv_n, float2* __restrict__ grad_ospec,
+    const float2* __restrict__ tw) {
+  using S = RegShape<N>;
+  using CP = ColPass<N>;
+  extern __shared__ float2 sm[];
+  const int tid = threadIdx.x;
+  const int c = tid % kColsPerCta;
+  const int t = tid / kColsPerCta;
+  constexpr int kSubs = kTile / kColsPerCta;
+  constexpr int kTiles = (N + kTile - 1) / kTile;
+  const int ct = blockIdx.x / kSubs;
+  const int c0 = ct * kTile + (blockIdx.x - ct * kSubs) * kColsPerCta;
+  const int f = blockIdx.y;
+  const int kc = c0 + c;
+  const bool col_ok = kc < N;
+  float2* tile = scratch + ((size_t)f * kTiles + ct) * N * kTile + (c0 - ct * kTile);
+  float2* buf = sm + c * CP::LP;
+  float2 v[S::N1];
+  const float dx = (STAGE == 1 || STAGE == 7) ? shifts[2 * f] : 0.f;
+  const float dy = (STAGE == 1 || STAGE == 7) ? shifts[2 * f + 1] : 0.f;
+  const int fx = signed_freq(kc, N);
+
+  if (STAGE == 1) {
+#pragma unroll
+    for (int j = 0; j < S::N1; ++j) {
+      const int kr = t + S::T * j;
+      float2 w = make_float2(0.f, 0.f);
+      if (col_ok) {
+        const size_t idx = (size_t)kr * N + kc;
+        w = cmul(ospec[idx], shift_ramp(dx, dy, fx, signed_freq(kr, N)));
+        if (t1) w = cmul(w, t1[idx]);
+      }
+      v[j] = w;
+    }
+    reg_fft<N, true, true>(v, buf, t, tw);
+  } else {
+#pragma unroll
+    for (int j = 0; j < S::N1; ++j) v[j] = col_ok ? tile[(t + S::T * j) * kTile + c] : make_float2(0.f, 0.f);
+    reg_fft<N, false, true>(v, buf, t, tw);
+    if (STAGE == 3) {
+#pragma unroll
+      for (int m = 0; m < S::N1; ++m) {
+        const int kr = t + S::T * m;
+        if (col_ok) {
+          const float2 h = t2[(size_t)kr * N + kc];
+          v[m] = CONJ ? cscale(cmulc(v[m], h), inv_n) : cmul(v[m], h);
+        }
+      }
+      reg_fft<N, true, true>(v, buf, t, tw);
+    } else {  // STAGE 7
+      if (col_ok) {
+#pragma unroll
+        for (int m = 0; m < S::N1; ++m) {
+          const int kr = t + S::T * m;
+          const size_t idx = (size_t)kr * N + kc;
+          float2 w = shift_ramp(dx, dy, fx, signed_freq(kr, N));
+          if (t1) w = cmul(w, t1[idx]);
+          atomicAdd(&grad_ospec[idx], cmulc(cscale(v[m], inv_n), w));
+        }
+      }
+      return;
+    }
+  }
+  if (col_ok) {
+#pragma unroll
+    for (int m = 0; m < S::N1; ++m) tile[(t + S::T * m) * kTile + c] = v[m];
+  }
+}
+
+// ---- row passes ------------------------------------------------------------------------
+
+template <int N>
+__device__ __forceinline__ void load_frame_row(const float2* __restrict__ scratch, int f, int r,
+                                               float2 (&v)[RegShape<N>::N1], int t) {
+  using S = RegShape<N>;
+  constexpr int kTiles = (N + kTile - 1) / kTile;
+  const float2* base = scratch + (size_t)f * kTiles * N * kTile + (size_t)r * kTile;
+#pragma unroll
+  for (int j = 0; j < S::N1; ++j) {
+    const int c = t + S::T * j;
+    v[j] = base[(size_t)(c / kTile) * N * kTile + (c % kTile)];
+  }
+}
+
+template <int N>
+__device__ __forceinline__ void store_frame_row(float2* __restrict__ scratch, int f, int r,
+                                                const float2 (&v)[RegShape<N>::N1], int t) {
+  using S = RegShape<N>;
+  constexpr int kTiles = (N + kTile - 1) / kTile;
+  float2* base = scratch + (size_t)f * kTiles * N * kTile + (size_t)r * kTile;
+#pragma unroll
+  for (int m = 0; m < S::N1; ++m) {
+    const int c = t + S::T * m;
+    base[(size_t)(c / kTile) * N * kTile + (c % kTile)] = v[m];
+  }
+}
+
+// Pass 2: inverse row DFT, x = ./n (stored), a = x M, forward row DFT.
+template <int N>
+__global__ void __launch_bounds__(256, 2) coded_rows_mask(float2* __restrict__ scratch,
+                                                          const float2* __restrict__ mask,
+                                                          float2* __restrict__ xstore, float inv_n,
+                                                          const float2* __restrict__ tw, int lines) {
+  using S = RegShape<N>;
+  extern __shared__ float2 sm[];
+  const int tid = threadIdx.x;
+  const int l = tid / S::T;
+  const int t = tid - l * S::T;
+  const int r = blockIdx.x * lines + l;
+  const int f = blockIdx.y;
+  const bool row_ok = r < N;
+  const int rr = row_ok ? r : 0;
+  float2 v[S::N1];
+  load_frame_row<N>(scratch, f, rr, v, t);
+  reg_fft<N, true, false>(v, sm + l * RowPass<N>::LP, t, tw);
+  float2* xrow = xstore + ((size_t)f * N + rr) * N;
+  const float2* mrow = mask + (size_t)rr * N;
+#pragma unroll
+  for (int m = 0; m < S::N1; ++m) {
+    const int c = t + S::T * m;
+    const float2 x = cscale(v[m], inv_n);
+    if (row_ok) xrow[c] = x;
+    v[m] = cmul(x, __ldg(&mrow[c]));
+  }
+  reg_fft<N, false, false>(v, sm + l * RowPass<N>::LP, t, tw);
+  if (row_ok) store_frame_row<N>(scratch, f, r, v, t);
+}
+
+// Pass 4.  kCodedSweep: inverse row DFT, s = ./n, RMS pool over ds x ds, FP64 loss,
+// g_s = gA / (A ds^2) s, forward row DFT.  kCodedForward: inverse row DFT, write s and
+// the pooled amplitude.  kCodedBackward: g_s from saved s, amplitude and grad_output,
+// forward row DFT.  A CTA owns `lines` consecutive rows, a multiple of ds.
+template <int MODE, int N>
+__global__ void __launch_bounds__(256, 2) coded_rows_pool(
+    float2* __restrict__ scratch, int ds, int frame0, float inv_n, const uint16_t* __restrict__ measured,
+    float scale, float grad_scale, double inv_numel, double* __restrict__ loss, float2* __restrict__ sensor,
+    float* __restrict__ amplitude, const float* __restrict__ grad_output, const float2* __restrict__ tw,
+    int lines) {
+  using S = RegShape<N>;
+  extern __shared__ float2 sm[];
+  float* pool = reinterpret_cast<float*>(sm + lines * RowPass<N>::LP);  // [lines][N] |s|^2, then factors
+  const int tid = threadIdx.x;
+  const int l = tid / S::T;
+  const int t = tid - l * S::T;
+  const int r0 = blockIdx.x * lines;
+  const int r = r0 + l;
+  const int f = blockIdx.y;
+  const size_t g = (size_t)frame0 + f;
+  const int lw = N / ds;  // pooled width
+  float2 v[S::N1];
+  if (MODE == kCodedBackward) {
+    const float2* srow = sensor + (g * N + r) * N;
+    const float* arow = amplitude + (g * lw + r / ds) * lw;
+    const float* grow = grad_output + (g * lw + r / ds) * lw;
+#pragma unroll
+    for (int m = 0; m < S::N1; ++m) {
+      const int c = t + S::T * m;
+      const float a = fmaxf(arow[c / ds], kAmpFloor);
+      v[m] = cscale(srow[c], grow[c / ds] / (a * static_cast<float>(ds * ds)));
+    }
+  } else {
+    load_frame_row<N>(scratch, f, r, v, t);
+    reg_fft<N, true, false>(v, sm + l * RowPass<N>::LP, t, tw);
+#pragma unroll
+    for (int m = 0; m < S::N1; ++m) {
+      v[m] = cscale(v[m], inv_n);
+      pool[l * N + t + S::T * m] = cabs2(v[m]);
+    }
+    __syncthreads();
+    // pooled values of this CTA: (lines/ds) x lw, one per thread-iteration
+    const int nb = (lines / ds) * lw;
+    double acc = 0.0;
+    for (int q = tid; q < nb; q += blockDim.x) {
+      const int py = q / lw, px = q - py * lw;
+      float sum = 0.f;
+      for (int yy = 0; yy < ds; ++yy)
+        for (int xx = 0; xx < ds; ++xx) sum += pool[(py * ds + yy) * N + px * ds + xx];
+      const float a = sqrtf(fmaxf(sum / static_cast<float>(ds * ds), 0.f));
+      const size_t oidx = (g * lw + r0 / ds + py) * lw + px;
+      if (MODE == kCodedForward) {
+        amplitude[oidx] = a;
+      } else {
+        const float y = sqrtf(static_cast<float>(measured[oidx]) * scale);
+        const float d = a - y;
+        acc += static_cast<double>(d) * static_cast<double>(d);
+        // store the factor gA / (A ds^2) at the block's first pixel
+        pool[(py * ds) * N + px * ds] = grad_scale * d / (fmaxf(a, kAmpFloor) * static_cast<float>(ds * ds));
+      }
+    }
+    if (MODE == kCodedForward) {
+      float2* srow = sensor + (g * N + r) * N;
+#pragma unroll
+      for (int m = 0; m < S::N1; ++m) srow[t + S::T * m] = v[m];
+      return;
+    }
+    block_add_double(acc, inv_numel, loss);  // synchronises the block
+#pragma unroll
+    for (int m = 0; m < S::N1; ++m) {
+      const int c = t + S::T * m;
+      v[m] = cscale(v[m], pool[((l / ds) * ds) * N + (c / ds) * ds]);
+    }
+  }
+  reg_fft<N, false, false>(v, sm + l * RowPass<N>::LP, t, tw);
+  store_frame_row<N>(scratch, f, r, v, t);
+}
+
+// Pass 6: inverse row DFT (g_a), grad_M += g_a conj(x) in registers over the CTA's frames,
+// g_a conj(M), forward row DFT.
+template <int N>
+__global__ void __launch_bounds__(128, 3) coded_rows_grad_mask(
+    float2* __restrict__ scratch, const float2* __restrict__ mask, const float2* __restrict__ xstore, int nframes,
+    int frames_per_cta, float2* __restrict__ grad_mask, const float2* __restrict__ tw, int lines) {
+  using S = RegShape<N>;
+  extern __shared__ float2 sm[];
+  const int tid = threadIdx.x;
+  const int l = tid / S::T;
+  const int t = tid - l * S::T;
+  const int r = blockIdx.x * lines + l;
+  const bool row_ok = r < N;
+  const int rr = row_ok ? r : 0;
+  const int f0 = blockIdx.y * frames_per_cta;
+  const int f1 = min(nframes, f0 + frames_per_cta);
+  float2* buf = sm + l * RowPass<N>::LP;
+  float2* xbuf = sm + lines * RowPass<N>::LP + l * N;
+  const float2* mrow = mask + (size_t)rr * N;
+  float2 acc[S::N1];
+#pragma unroll
+  for (int m = 0; m < S::N1; ++m) acc[m] = make_float2(0.f, 0.f);
+  for (int f = f0; f < f1; ++f) {
+    const float2* xrow = xstore + ((size_t)f * N + rr) * N;
+#pragma unroll
+    for (int m = 0; m < S::N1; ++m) cp_async8(xbuf + t + S::T * m, xrow + t + S::T * m);
+    cp_async_commit();
+    float2 v[S::N1];
+    load_frame_row<N>(scratch, f, rr, v, t);
+    reg_fft<N, true, false>(v, buf, t, tw);
+    cp_async_wait_all();
+#pragma unroll
+    for (int m = 0; m < S::N1; ++m) {
+      const int c = t + S::T * m;
+      acc[m] = cadd(acc[m], cmulc(v[m], xbuf[c]));
+      v[m] = cmulc(v[m], __ldg(&mrow[c]));
+    }
+    reg_fft<N, false, false>(v, buf, t, tw);
+    if (row_ok) store_frame_row<N>(scratch, f, r, v, t);
+  }
+  if (row_ok) {
+#pragma unroll
+    for (int m = 0; m < S::N1; ++m) atomicAdd(&grad_mask[(size_t)r * N + t + S::T * m], acc[m]);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------------------
+
+struct CodedGeom {
+  int n, ds, batch;
+  LinePlan plan;
+  size_t field_bytes;
+  int chunk;
+  float2* ospec;
+  float2* gospec;
+  float2* tmp;
+  float2* xstore;
+  float2* frames;
+};
+
+size_t coded_fixed_bytes(int n) { return kHdr + 3 * (size_t)n * n * sizeof(float2); }
+
+int coded_lines(int n) {
+  int lines = 0;
+  dispatch_pow2(n, [&](auto NT) {
+    constexpr int N = decltype(NT)::value;
+    lines = RowPass<N>::lines(256, N);
+  });
+  return lines;
+}
+
+int coded_check(int n, int ds, const void* a, const void* b, const void* t2, const float* shifts, int batch, void* ws,
+                size_t ws_bytes, bool need_xstore, CodedGeom* g) {
+  if (!a || !b || !t2 || (!shifts && batch > 0) || !ws) return set_error(PTX_ERR_INVALID_ARGUMENT, "null pointer argument");
+  if (batch < 0) return set_error(PTX_ERR_INVALID_ARGUMENT, "negative batch");
+  if (!is_pow2_len(n) || n < 16) {
+    return set_error(PTX_ERR_UNSUPPORTED_SIZE, "coded field side must be a power of two in [16, 1024] (got %d)", n);
+  }
+  const int lines = coded_lines(n);
+  if (ds < 1 || n % ds != 0 || lines % ds != 0) {
+    return set_error(PTX_ERR_UNSUPPORTED_SIZE, "downsample %d must divide %d and %d", ds, n, lines);
+  }
+  g->n = n; g->ds = ds; g->batch = batch;
+  if (int st = get_line_plan(n, &g->plan)) return st;
+  g->field_bytes = (size_t)n * n * sizeof(float2);
+  const size_t fixed = coded_fixed_bytes(n);
+  const size_t per = g->field_bytes * (need_xstore ? 2 : 1);
+  if (ws_bytes < fixed + per) {
+    return set_error(PTX_ERR_WORKSPACE, "workspace of %zu bytes is smaller than the %zu bytes needed", ws_bytes,
+                     fixed + per);
+  }
+  g->chunk = static_cast<int>(std::min<size_t>((ws_bytes - fixed) / per, (size_t)std::max(batch, 1)));
+  char* p = static_cast<char*>(ws) + kHdr;
+  g->ospec = reinterpret_cast<float2*>(p);
+  g->gospec = reinterpret_cast<float2*>(p + g->field_bytes);
+  g->tmp = reinterpret_cast<float2*>(p + 2 * g->field_bytes);
+  g->frames = reinterpret_cast<float2*>(p + 3 * g->field_bytes);
+  g->xstore = need_xstore ? reinterpret_cast<float2*>(p + 3 * g->field_bytes + (size_t)g->chunk * g->field_bytes)
+                          : nullptr;
+  int st = PTX_OK;
+  dispatch_pow2(n, [&](auto NT) {
+    constexpr int N = decltype(NT)::value;
+    const int rs = RowPass<N>::smem(lines);
+    const int rs_row = RowPass<N>::smem_with_row(RowPass<N>::lines(128, N));
+    const int pool = rs + lines * N * (int)sizeof(float);
+    const int cs = kColsPerCta * ColPass<N>::LP * (int)sizeof(float2);
+    if (!st) st = ensure_smem((const void*)fft2_rows_kernel<N, false>, rs);
+    if (!st) st = ensure_smem((const void*)fft2_rows_kernel<N, true>, rs);
+    if (!st) st = ensure_smem((const void*)fft2_cols_kernel<N, false>, cs);
+    if (!st) st = ensure_smem((const void*)fft2_cols_kernel<N, true>, cs);
+    if (!st) st = ensure_smem((const void*)coded_cols<1, false, N>, cs);
+    if (!st) st = ensure_smem((const void*)coded_cols<3, false, N>, cs);
+    if (!st) st = ensure_smem((const void*)coded_cols<3, true, N>, cs);
+    if (!st) st = ensure_smem((const void*)coded_cols<7, false, N>, cs);
+    if (!st) st = ensure_smem((const void*)coded_rows_mask<N>, rs);
+    if (!st) st = ensure_smem((const void*)coded_rows_pool<kCodedSweep, N>, pool);
+    if (!st) st = ensure_smem((const void*)coded_rows_pool<kCodedForward, N>, pool);
+    if (!st) st = ensure_smem((const void*)coded_rows_pool<kCodedBackward, N>, pool);
+    if (!st) st = ensure_smem((const void*)coded_rows_grad_mask<N>, rs_row);
+  });
+  return st;
+}
+
+template <bool INV>
+void launch_fft2(const float2* in, int n, float2* out, float2* tmp, const LinePlan& p, cudaStream_t s) {
+  dispatch_pow2(n, [&](auto NT) {
+    constexpr int N = decltype(NT)::value;
+    const int lines = RowPass<N>::lines(256, N);
+    prof_begin(kFft2Rows, s);
+    fft2_rows_kernel<N, INV><<<(N + lines - 1) / lines, lines * RowPass<N>::T, RowPass<N>::smem(lines), s>>>(
+        in, N, tmp, p.tw, lines);
+    prof_end(kFft2Rows, s);
+    prof_begin(kFft2Cols, s);
+    fft2_cols_kernel<N, INV><<<num_tiles(N) * (kTile / kColsPerCta), ColPass<N>::kThreads,
+                               kColsPerCta * ColPass<N>::LP * (int)sizeof(float2), s>>>(tmp, N, out, 1.0f, p.tw);
+    prof_end(kFft2Cols, s);
+  });
+}
+
+template <int STAGE, bool CONJ>
+void launch_cols(const CodedGeom& g, int nf, const float2* t1, const float2* t2, const float* shifts,
+                 cudaStream_t s) {
+  const float inv_n = 1.0f / static_cast<float>((double)g.n * g.n);
+  prof_begin(kCodedCols, s);
+  dispatch_pow2(g.n, [&](auto NT) {
+    constexpr int N = decltype(NT)::value;
+    dim3 grid(num_tiles(N) * (kTile / kColsPerCta), nf);
+    coded_cols<STAGE, CONJ, N><<<grid, ColPass<N>::kThreads, kColsPerCta * ColPass<N>::LP * (int)sizeof(float2), s>>>(
+        g.frames, g.ospec, t1, t2, shifts, inv_n, g.gospec, g.plan.tw);
+  });
+  prof_end(kCodedCols, s);
+}
+
+void launch_rows_mask(const CodedGeom& g, int nf, const float2* mask, float2* xstore, cudaStream_t s) {
+  const float inv_n = 1.0f / static_cast<float>((double)g.n * g.n);
+  prof_begin(kCodedRows, s);
+  dispatch_pow2(g.n, [&](auto NT) {
+    constexpr int N = decltype(NT)::value;
+    const int lines = RowPass<N>::lines(256, N);
+    dim3 grid((N + lines - 1) / lines, nf);
+    coded_rows_mask<N><<<grid, lines * RowPass<N>::T, RowPass<N>::smem(lines), s>>>(g.frames, mask, xstore, inv_n,
+                                                                                   g.plan.tw, lines);
+  });
+  prof_end(kCodedRows, s);
+}
+
+template <int MODE>
+void launch_rows_pool(const CodedGeom& g, int frame0, int nf, const uint16_t* measured, float scale,
+                      float grad_scale, double inv_numel, double* loss, float2* sensor, float* amplitude,
+                      const float* grad_output, cudaStream_t s) {
+  const float inv_n = 1.0f / static_cast<float>((double)g.n * g.n);
+  prof_begin(kCodedRows, s);
+  dispatch_pow2(g.n, [&](auto NT) {
+    constexpr int N = decltype(NT)::value;
+    const int lines = RowPass<N>::lines(256, N);
+    dim3 grid((N + lines - 1) / lines, nf);
+    const int smem = RowPass<N>::smem(lines) + lines * N * (int)sizeof(float);
+    coded_rows_pool<MODE, N><<<grid, lines * RowPass<N>::T, smem, s>>>(g.frames, g.ds, frame0, inv_n, measured, scale,
+                                                                       grad_scale, inv_numel, loss, sensor, amplitude,
+                                                                       grad_output, g.plan.tw, lines);
+  });
+  prof_end(kCodedRows, s);
+}
+
+void launch_rows_grad_mask(const CodedGeom& g, int nf, const float2* mask, const float2* xstore, float2* grad_mask,
+                           cudaStream_t s) {
+  prof_begin(kCodedRows, s);
+  dispatch_pow2(g.n, [&](auto NT) {
+    constexpr int N = decltype(NT)::value;
+    const int lines = RowPass<N>::lines(128, N);
+    const int rowgroups = (N + lines - 1) / lines;
+    const long long ctas_one = (long long)rowgroups * nf;
+    const int fpc = std::max(1, std::min<int>(nf, static_cast<int>(ctas_one / (sm_count() * 6))));
+    dim3 grid(rowgroups, (nf + fpc - 1) / fpc);
+    coded_rows_grad_mask<N><<<grid, lines * RowPass<N>::T, RowPass<N>::smem_with_row(lines), s>>>(
+        g.frames, mask, xstore, nf, fpc, grad_mask, g.plan.tw, lines);
+  });
+  prof_end(kCodedRows, s);
+}
+
+// The adjoint passes 4 (backward part) to 7 for one chunk, given g_s already in the frames.
+void adjoint_tail(const CodedGeom& g, int nf, const float2* mask, const float2* t1, const float2* t2,
+                  const float* shifts, const float2* xstore, float2* grad_mask, cudaStream_t s) {
+  launch_cols<3, true>(g, nf, t1, t2, shifts, s);
+  launch_rows_grad_mask(g, nf, mask, xstore, grad_mask, s);
+  launch_cols<7, false>(g, nf, t1, t2, shifts, s);
+}
+
+}  // namespace
+}  // namespace ptx
+
+using namespace ptx;
+
+extern "C" {
+
+size_t ptx_coded_workspace_bytes(int n, int batch) {
+  if (n <= 0) return 0;
+  const size_t field = (size_t)n * n * sizeof(float2);
+  const size_t frames = std::max<size_t>(1, std::min<size_t>((size_t)std::max(batch, 1), (4096ull << 20) / (2 * field)));
+  return coded_fixed_bytes(n) + frames * 2 * field;
+}
+
+int ptx_coded_forward(const float* object, const float* coded_surface, const float* transfer_1, const float* transfer_2,
+                      int n, const float* shifts_xy, int batch, int downsample, float* x_forward, float* sensor,
+                      float* amplitude, void* workspace, size_t workspace_bytes, void* stream) {
+  CodedGeom g;
+  if (int st = coded_check(n, downsample, object, coded_surface, transfer_2, shifts_xy, batch, workspace,
+                           workspace_bytes, false, &g)) {
+    return st;
+  }
+  if ((!x_forward || !sensor || !amplitude) && batch > 0) return set_error(PTX_ERR_INVALID_ARGUMENT, "null output");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const float2* T1 = reinterpret_cast<const float2*>(transfer_1);
+  const float2* T2 = reinterpret_cast<const float2*>(transfer_2);
+  const float2* M = reinterpret_cast<const float2*>(coded_surface);
+  launch_fft2<false>(reinterpret_cast<const float2*>(object), n, g.ospec, g.tmp, g.plan, s);
+  for (int b0 = 0; b0 < batch; b0 += g.chunk) {
+    const int nf = std::min(g.chunk, batch - b0);
+    const float* sh = shifts_xy + 2 * (size_t)b0;
+    launch_cols<1, false>(g, nf, T1, T2, sh, s);
+    launch_rows_mask(g, nf, M, reinterpret_cast<float2*>(x_forward) + (size_t)b0 * n * n, s);
+    launch_cols<3, false>(g, nf, T1, T2, sh, s);
+    launch_rows_pool<kCodedForward>(g, b0, nf, nullptr, 0.f, 0.f, 0.0, nullptr, reinterpret_cast<float2*>(sensor),
+                                    amplitude, nullptr, s);
+  }
+  return cuda_status(cudaGetLastError(), "ptx_coded_forward launch");
+}
+
+int ptx_coded_backward(const float* grad_output, const float* x_forward, const float* sensor, const float* amplitude,
+                       const float* coded_surface, const float* transfer_1, const float* transfer_2, int n,
+                       const float* shifts_xy, int batch, int downsample, float* grad_object, float* grad_coded,
+                       void* workspace, size_t workspace_bytes, void* stream) {
+  CodedGeom g;
+  if (int st = coded_check(n, downsample, coded_surface, coded_surface, transfer_2, shifts_xy, batch, workspace,
+                           workspace_bytes, false, &g)) {
+    return st;
+  }
+  if (((!grad_output || !x_forward || !sensor || !amplitude) && batch > 0) || !grad_object || !grad_coded) {
+    return set_error(PTX_ERR_INVALID_ARGUMENT, "null pointer argument");
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const float2* T1 = reinterpret_cast<const float2*>(transfer_1);
+  const float2* T2 = reinterpret_cast<const float2*>(transfer_2);
+  const float2* M = reinterpret_cast<const float2*>(coded_surface);
+  cudaMemsetAsync(g.gospec, 0, g.field_bytes, s);
+  cudaMemsetAsync(grad_coded, 0, g.field_bytes, s);
+  for (int b0 = 0; b0 < batch; b0 += g.chunk) {
+    const int nf = std::min(g.chunk, batch - b0);
+    launch_rows_pool<kCodedBackward>(g, b0, nf, nullptr, 0.f, 0.f, 0.0, nullptr,
+                                     const_cast<float2*>(reinterpret_cast<const float2*>(sensor)),
+                                     const_cast<float*>(amplitude), grad_output, s);
+    adjoint_tail(g, nf, M, T1, T2, shifts_xy + 2 * (size_t)b0,
+                 reinterpret_cast<const float2*>(x_forward) + (size_t)b0 * n * n,
+                 reinterpret_cast<float2*>(grad_coded), s);
+  }
+  launch_fft2<true>(g.gospec, n, reinterpret_cast<float2*>(grad_object), g.tmp, g.plan, s);
+  return cuda_status(cudaGetLastError(), "ptx_coded_backward launch");
+}
+
+int ptx_coded_sweep(const float* object, const float* coded_surface, const float* transfer_1, const float* transfer_2,
+                    int n, const float* shifts_xy, int batch, int downsample, const uint16_t* measured, float scale,
+                    double* loss, float* grad_object, float* grad_coded, void* workspace, size_t workspace_bytes,
+                    void* stream) {
+  CodedGeom g;
+  if (int st = coded_check(n, downsample, object, coded_surface, transfer_2, shifts_xy, batch, workspace,
+                           workspace_bytes, true, &g)) {
+    return st;
+  }
+  if ((!measured && batch > 0) || !loss || !grad_object || !grad_coded) {
+    return set_error(PTX_ERR_INVALID_ARGUMENT, "null pointer argument");
+  }
+  if (!(scale > 0.f)) return set_error(PTX_ERR_INVALID_ARGUMENT, "scale must be positive");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const float2* T1 = reinterpret_cast<const float2*>(transfer_1);
+  const float2* T2 = reinterpret_cast<const float2*>(transfer_2);
+  const float2* M = reinterpret_cast<const float2*>(coded_surface);
+  cudaMemsetAsync(g.gospec, 0, g.field_bytes, s);
+  cudaMemsetAsync(grad_coded, 0, g.field_bytes, s);
+  cudaMemsetAsync(loss, 0, sizeof(double), s);
+  const int lw = n / downsample;
+  const double numel = (double)batch * lw * lw;
+  const float grad_scale = static_cast<float>(2.0 / std::max(numel, 1.0));
+  launch_fft2<false>(reinterpret_cast<const float2*>(object), n, g.ospec, g.tmp, g.plan, s);
+  for (int b0 = 0; b0 < batch; b0 += g.chunk) {
+    const int nf = std::min(g.chunk, batch - b0);
+    const float* sh = shifts_xy + 2 * (size_t)b0;
+    launch_cols<1, false>(g, nf, T1, T2, sh, s);
+    launch_rows_mask(g, nf, M, g.xstore, s);
+    launch_cols<3, false>(g, nf, T1, T2, sh, s);
+    launch_rows_pool<kCodedSweep>(g, b0, nf, measured, scale, grad_scale, 1.0 / std::max(numel, 1.0), loss, nullptr,
+                                  nullptr, nullptr, s);
+    adjoint_tail(g, nf, M, T1, T2, sh, g.xstore, reinterpret_cast<float2*>(grad_coded), s);
+  }
+  launch_fft2<true>(g.gospec, n, reinterpret_cast<float2*>(grad_object), g.tmp, g.plan, s);
+  return cuda_status(cudaGetLastError(), "ptx_coded_sweep launch");
+}
+
+}  // extern "C"
