@@ -44,25 +44,6 @@ FALLBACK_HBM_GBS = 6650.0
 # workloads
 # ---------------------------------------------------------------------------------------
 
-WORKLOADS = {
-    # name: (object side, probe side, raster grid, step, origin, jitter, photons)
-    "conventional-900x512-2048": (2048, 512, 30, 48, 64, 3, 1e5),
-    "conventional-121x128-512": (512, 128, 11, 32, 8, 2, 1e4),
-}
-DEFAULT_WORKLOAD = "conventional-900x512-2048"
-
-
-def conventional_bytes_model(n_obj: int, p: int, batch: int) -> float:
-    """Algorithmic HBM bytes of one conventional sweep.
-
-    Per position: 8 P^2 (object window gather) + 2 P^2 (uint16 counts) + 16 P^2
-    (object-gradient read-modify-write); per sweep: + 16 P^2 (probe in, probe gradient
-    out) + 8 N^2 (zeroing the object gradient).
-    """
-    p2 = float(p) * p
-    return 26.0 * p2 * batch + 16.0 * p2 + 8.0 * float(n_obj) ** 2
-
-
 def hbm_peak() -> tuple[float, str]:
     try:
         d = json.loads(MEASURED_PEAKS.read_text())
@@ -71,42 +52,266 @@ def hbm_peak() -> tuple[float, str]:
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def synth_conventional(name: str, seed: int, device):
-    """Seeded cfg inputs: truth -> CUDA forward -> Poisson counts; evaluation point = perturbed truth."""
+class Workload:
+    """One benchmark configuration: synthesis, fused sweep, public-API step, byte model."""
+
+    name = ""
+    units = "positions"
+
+    def metric(self) -> str:
+        raise NotImplementedError
+
+    def bytes_per_sweep(self) -> float:
+        raise NotImplementedError
+
+    def config(self) -> dict:
+        raise NotImplementedError
+
+
+class Conventional(Workload):
+    """Raster-scanned conventional ptychography (configs 0 and 1)."""
+
+    def __init__(self, name, n_obj, p, grid, step, origin, jitter, photons):
+        self.name, self.n_obj, self.p = name, n_obj, p
+        self.grid, self.step, self.origin, self.jitter, self.photons = grid, step, origin, jitter, photons
+        self.batch = grid * grid
+
+    def metric(self):
+        return f"fwd+adj sweeps/s ({self.batch}×{self.p}²→{self.n_obj}²)"
+
+    def bytes_per_sweep(self):
+        # per position 8 P^2 gather + 2 P^2 counts + 16 P^2 grad_O RMW; + 16 P^2 + 8 N^2 per sweep
+        p2 = float(self.p) ** 2
+        return 26.0 * p2 * self.batch + 16.0 * p2 + 8.0 * float(self.n_obj) ** 2
+
+    def config(self):
+        return {"workload": self.name, "modality": "conventional", "positions": self.batch,
+                "probe": [self.p, self.p], "object": [self.n_obj, self.n_obj],
+                "raster": f"{self.grid}x{self.grid} step {self.step} origin {self.origin} jitter U[-{self.jitter},{self.jitter}]",
+                "photons_per_pattern": self.photons}
+
+    def host(self, seed):
+        from ptychox_b200 import synth
+
+        rng = np.random.default_rng(seed)
+        obj = synth.random_object(self.n_obj, self.n_obj, rng)
+        probe = synth.gaussian_probe(self.p, self.p, rng)
+        pos = synth.raster_positions(self.grid, self.step, self.origin, self.jitter, rng)
+        guess = (obj * (1 + 0.1 * rng.standard_normal(obj.shape))).astype(np.complex64)
+        return {"truth": obj, "obj": guess, "aux": probe, "pos": pos}
+
+    def synth(self, seed, dev):
+        import torch
+
+        from ptychox_b200 import ptychoX_base
+
+        h = self.host(seed)
+        with torch.no_grad():
+            amp = ptychoX_base(torch.from_numpy(h["truth"]).to(dev), torch.from_numpy(h["aux"]).to(dev),
+                               torch.from_numpy(h["pos"]).to(dev))
+            meas, scale = device_poisson(amp, self.photons, seed, per_pixel=False)
+        return self._pack(h, meas, scale, dev)
+
+    def _pack(self, h, meas, scale, dev):
+        import torch
+
+        return {"obj": torch.from_numpy(h["obj"]).to(dev), "aux": torch.from_numpy(h["aux"]).to(dev),
+                "pos": torch.from_numpy(h["pos"]).to(dev), "meas": meas, "scale": scale, "host": h}
+
+    def workspace(self, prob, dev):
+        from ptychox_b200 import _abi
+        from ptychox_b200._utils import workspace
+
+        return workspace(_abi.query("ptx_base_workspace_bytes", self.p, self.p, self.batch), dev)
+
+    def sweep(self, prob, ws):
+        from ptychox_b200.base import base_sweep
+
+        return base_sweep(prob["obj"], prob["aux"], prob["pos"], prob["meas"], prob["scale"], ws=ws)
+
+    def loss_api(self, obj, aux, pos, prob):
+        from ptychox_b200 import ptychoX_base_loss
+
+        return ptychoX_base_loss(obj, aux, pos, prob["meas"], prob["scale"])
+
+    def cpu_sweep(self, h, meas, scale, k, workers):
+        from oracle import ptycho_oracle as O
+
+        O.base_sweep(h["obj"], h["aux"], h["pos"][:k], meas[:k], scale, fp64=False, workers=workers)
+
+
+class Fourier(Conventional):
+    """Fourier ptychography (config 2): 15x15 LEDs, 256^2 pupil, 1024^2 spectrum."""
+
+    def __init__(self, name, n, h, grid, photons):
+        self.name, self.n_obj, self.p, self.grid, self.photons = name, n, h, grid, photons
+        self.batch = grid * grid
+
+    def metric(self):
+        return f"fwd+adj sweeps/s (FPM {self.batch}×{self.p}²←{self.n_obj}²)"
+
+    def bytes_per_sweep(self):
+        # per LED 26 h^2; per sweep + 72 N^2 (spectrum and gradient transforms) + 16 h^2
+        h2 = float(self.p) ** 2
+        return 26.0 * h2 * self.batch + 72.0 * float(self.n_obj) ** 2 + 16.0 * h2
+
+    def config(self):
+        return {"workload": self.name, "modality": "fourier", "leds": self.batch, "pupil": [self.p, self.p],
+                "object": [self.n_obj, self.n_obj], "na": 0.1, "wavelength_um": 0.532, "led_pitch_mm": 4.0,
+                "led_height_mm": 90.0, "photons_per_pixel_brightest": self.photons}
+
+    def host(self, seed):
+        from ptychox_b200 import synth
+
+        rng = np.random.default_rng(seed)
+        obj = synth.random_object(self.n_obj, self.n_obj, rng)
+        pupil = synth.circular_pupil(self.p, 0.3)
+        dx = synth.fpm_dx_for_pupil(self.n_obj, self.p, 0.1, 0.532, 0.3)
+        led = synth.fpm_led_windows(self.n_obj, self.p, self.grid, 4.0, 90.0, 0.532, dx)
+        guess = (obj * (1 + 0.1 * rng.standard_normal(obj.shape))).astype(np.complex64)
+        return {"truth": obj, "obj": guess, "aux": pupil, "pos": led}
+
+    def synth(self, seed, dev):
+        import torch
+
+        from ptychox_b200 import ptychoX_fourier
+
+        h = self.host(seed)
+        with torch.no_grad():
+            amp = ptychoX_fourier(torch.from_numpy(h["truth"]).to(dev), torch.from_numpy(h["aux"]).to(dev),
+                                  torch.from_numpy(h["pos"]).to(dev))
+            meas, scale = device_poisson(amp, self.photons, seed, per_pixel=True, brightest=True)
+        return self._pack(h, meas, scale, dev)
+
+    def workspace(self, prob, dev):
+        from ptychox_b200 import _abi
+        from ptychox_b200._utils import workspace
+
+        return workspace(_abi.query("ptx_fpm_workspace_bytes", self.n_obj, self.n_obj, self.p, self.p, self.batch),
+                         dev)
+
+    def sweep(self, prob, ws):
+        from ptychox_b200.fpm import fpm_sweep
+
+        return fpm_sweep(prob["obj"], prob["aux"], prob["pos"], prob["meas"], prob["scale"], ws=ws)
+
+    def loss_api(self, obj, aux, pos, prob):
+        from ptychox_b200 import ptychoX_fourier_loss
+
+        return ptychoX_fourier_loss(obj, aux, pos, prob["meas"], prob["scale"])
+
+    def cpu_sweep(self, h, meas, scale, k, workers):
+        from oracle import ptycho_oracle as O
+
+        O.fpm_sweep(h["obj"], h["aux"], h["pos"][:k], meas[:k], scale, fp64=False, workers=workers)
+
+
+class Coded(Conventional):
+    """Coded / near-field ptychography (config 3): 1024^2 field, 64 shifts, ds 4."""
+
+    def __init__(self, name, n, count, ds, photons, nearfield):
+        self.name, self.n_obj, self.batch, self.ds, self.photons = name, n, count, ds, photons
+        self.nearfield = nearfield
+        self.p = n
+
+    def metric(self):
+        kind = "near-field" if self.nearfield else "coded"
+        return f"fwd+adj sweeps/s ({kind} {self.batch}×{self.n_obj}², ds {self.ds})"
+
+    def bytes_per_sweep(self):
+        n2 = float(self.n_obj) ** 2
+        return 240.125 * n2 * self.batch + 64.0 * n2
+
+    def config(self):
+        return {"workload": self.name, "modality": "near-field" if self.nearfield else "coded",
+                "positions": self.batch, "field": [self.n_obj, self.n_obj], "downsample": self.ds,
+                "pixel_um": 1.85, "wavelength_um": 0.5, "z_mm": 2.0,
+                "z1_um": None if self.nearfield else 396.95, "mask": "binary 50% fill",
+                "shifts_px": "U[-20, 20]", "photons_per_pixel": self.photons}
+
+    def host(self, seed):
+        from ptychox_b200 import synth
+
+        rng = np.random.default_rng(seed)
+        n = self.n_obj
+        obj = synth.random_object(n, n, rng)
+        mask = synth.binary_mask(n, 0.5, rng)
+        t2 = synth.angular_spectrum_transfer(n, 1.85e-6, 0.5e-6, 2e-3)
+        t1 = None if self.nearfield else synth.angular_spectrum_transfer(n, 1.85e-6, 0.5e-6, 396.95e-6)
+        shifts = synth.coded_shifts(self.batch, 20.0, n, rng)
+        guess = (obj * (1 + 0.1 * rng.standard_normal(obj.shape))).astype(np.complex64)
+        return {"truth": obj, "obj": guess, "aux": mask, "pos": shifts, "t1": t1, "t2": t2}
+
+    def synth(self, seed, dev):
+        import torch
+
+        from ptychox_b200 import ptychoX_coded, ptychoX_nearfield
+
+        h = self.host(seed)
+        t = lambda a: None if a is None else torch.from_numpy(a).to(dev)  # noqa: E731
+        with torch.no_grad():
+            if self.nearfield:
+                amp = ptychoX_nearfield(t(h["truth"]), t(h["aux"]), t(h["t2"]), t(h["pos"]), self.ds)
+            else:
+                amp = ptychoX_coded(t(h["truth"]), t(h["aux"]), t(h["t1"]), t(h["t2"]), t(h["pos"]), self.ds)
+            meas, scale = device_poisson(amp, self.photons, seed, per_pixel=True)
+        prob = self._pack(h, meas, scale, dev)
+        prob["t1"], prob["t2"] = t(h["t1"]), t(h["t2"])
+        return prob
+
+    def workspace(self, prob, dev):
+        from ptychox_b200 import _abi
+        from ptychox_b200._utils import workspace
+
+        return workspace(_abi.query("ptx_coded_workspace_bytes", self.n_obj, self.batch), dev)
+
+    def sweep(self, prob, ws):
+        from ptychox_b200.coded import coded_sweep
+
+        return coded_sweep(prob["obj"], prob["aux"], prob["t1"], prob["t2"], prob["pos"], self.ds, prob["meas"],
+                           prob["scale"], ws=ws)
+
+    def loss_api(self, obj, aux, pos, prob):
+        from ptychox_b200 import ptychoX_coded_loss, ptychoX_nearfield_loss
+
+        if self.nearfield:
+            return ptychoX_nearfield_loss(obj, aux, prob["t2"], pos, self.ds, prob["meas"], prob["scale"])
+        return ptychoX_coded_loss(obj, aux, prob["t1"], prob["t2"], pos, self.ds, prob["meas"], prob["scale"])
+
+    def cpu_sweep(self, h, meas, scale, k, workers):
+        from oracle import ptycho_oracle as O
+
+        O.coded_sweep(h["obj"], h["aux"], h["t1"], h["t2"], h["pos"][:k], self.ds, meas[:k], scale, fp64=False,
+                      workers=workers)
+
+
+WORKLOADS = {
+    w.name: w
+    for w in [
+        Conventional("conventional-900x512-2048", 2048, 512, 30, 48, 64, 3, 1e5),
+        Conventional("conventional-121x128-512", 512, 128, 11, 32, 8, 2, 1e4),
+        Fourier("fourier-225x256-1024", 1024, 256, 15, 5e3),
+        Coded("coded-64x1024-ds4", 1024, 64, 4, 2e3, nearfield=False),
+        Coded("nearfield-64x1024-ds4", 1024, 64, 4, 2e3, nearfield=True),
+    ]
+}
+DEFAULT_WORKLOAD = "conventional-900x512-2048"
+
+
+def device_poisson(amp, photons, seed, per_pixel=False, brightest=False):
+    """uint16 Poisson counts of amp^2 / scale on the device (scale as synth.poisson_counts)."""
     import torch
 
-    from ptychox_b200 import ptychoX_base, synth
-
-    n_obj, p, grid, step, origin, jitter, photons = WORKLOADS[name]
-    rng = np.random.default_rng(seed)
-    obj_true = synth.random_object(n_obj, n_obj, rng)
-    probe = synth.gaussian_probe(p, p, rng)
-    pos = synth.raster_positions(grid, step, origin, jitter, rng)
-    s = torch.from_numpy(obj_true).to(device)
-    pr = torch.from_numpy(probe).to(device)
-    pd = torch.from_numpy(pos).to(device)
-    with torch.no_grad():
-        amp = ptychoX_base(s, pr, pd)
-        inten = amp.double() ** 2
-        scale = float(np.float32(float(inten.sum(dim=(1, 2)).mean()) / photons))
-        gen = torch.Generator(device=device).manual_seed(seed)
-        counts = torch.poisson(inten / scale, generator=gen)
-        if float(counts.max()) > 65535:
-            raise RuntimeError("synthetic counts saturate uint16")
-        meas = counts.to(torch.int32).to(torch.uint16)
-        del amp, inten, counts
-    guess = (obj_true * (1 + 0.1 * rng.standard_normal(obj_true.shape))).astype(np.complex64)
-    return {
-        "sample": torch.from_numpy(guess).to(device),
-        "probe": pr,
-        "positions": pd,
-        "measured": meas,
-        "scale": scale,
-        "host": {"sample": guess, "probe": probe, "positions": pos},
-        "n_obj": n_obj,
-        "p": p,
-        "batch": len(pos),
-    }
+    inten = amp.double() ** 2
+    sums = inten.flatten(1).sum(dim=1)
+    per_pattern = float(sums.max() if brightest else sums.mean())
+    denom = photons * (inten[0].numel() if per_pixel else 1)
+    scale = float(np.float32(per_pattern / denom))
+    gen = torch.Generator(device=amp.device).manual_seed(seed)
+    counts = torch.poisson(inten / scale, generator=gen)
+    if float(counts.max()) > 65535:
+        raise RuntimeError("synthetic counts saturate uint16")
+    return counts.to(torch.int32).to(torch.uint16), scale
 
 
 # ---------------------------------------------------------------------------------------
@@ -172,10 +377,9 @@ def run_ours(args) -> None:
     import torch
     import torch.distributed as dist
 
-    from ptychox_b200 import _abi, ptychoX_base_loss
-    from ptychox_b200.base import base_sweep
-    from ptychox_b200._utils import workspace
+    from ptychox_b200 import _abi
 
+    wl = WORKLOADS[args.workload]
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -187,23 +391,20 @@ def run_ours(args) -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     _abi.load()
 
-    prob = synth_conventional(args.workload, seed=1000 + rank, device=dev)
-    s, pr, pos, meas, scale = prob["sample"], prob["probe"], prob["positions"], prob["measured"], prob["scale"]
-    ph = pw = prob["p"]
-    batch = prob["batch"]
-    ws = workspace(_abi.query("ptx_base_workspace_bytes", ph, pw, batch), dev)
+    prob = wl.synth(seed=1000 + rank, dev=dev)
+    ws = wl.workspace(prob, dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
     def step():
-        loss, gs, gp = base_sweep(s, pr, pos, meas, scale, ws=ws)
-        if world > 1:
-            dist.all_reduce(gs)
-            dist.all_reduce(gp)
+        loss, g_obj, g_aux = wl.sweep(prob, ws)
+        if world > 1:  # data-parallel sweep: sum the ranks' gradients
+            dist.all_reduce(g_obj)
+            dist.all_reduce(g_aux)
             dist.all_reduce(loss)
         return loss
 
     def timed(k: int, fn) -> list[float]:
-        times = []
+        pairs = []
         stream = torch.cuda.current_stream(dev)
         for _ in range(k):
             a = torch.cuda.Event(enable_timing=True)
@@ -212,17 +413,25 @@ def run_ours(args) -> None:
             fn()
             b.record(stream)
             flush.zero_()  # write > L2 between timed steps (outside the events)
-            times.append((a, b))
+            pairs.append((a, b))
         torch.cuda.synchronize(dev)
-        return [a.elapsed_time(b) for a, b in times]
+        return [a.elapsed_time(b) for a, b in pairs]
 
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    clocks = ClockSampler(local)
+    clocks.start()  # sampling runs from the warm-up through the timed region (200 ms period)
+    time.sleep(0.5)
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize(dev)
 
     # ---- timed region -------------------------------------------------------------
-    clocks = ClockSampler(local)
-    clocks.start()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize(dev)
@@ -233,11 +442,7 @@ def run_ours(args) -> None:
     if world > 1:
         dist.barrier()
     clk = clocks.stop()
-    total_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(sum(step_ms))
     ms_per_step = total_ms / args.steps
     value = world * args.steps / (total_ms / 1e3)
 
@@ -247,15 +452,12 @@ def run_ours(args) -> None:
     prof_ms = timed(args.steps, step)
     _abi.query("ptx_profile_enable", 0)
     per_kernel = _abi.profile_read()
-    sweep_bytes = conventional_bytes_model(prob["n_obj"], ph, batch)
     peak, peak_kind = hbm_peak()
-    sweep_ms = statistics.median(prof_ms)
+    sweep_bytes = wl.bytes_per_sweep()
     achieved = sweep_bytes / (ms_per_step / 1e3) / 1e9
-    kernels = []
     kern_total = sum(v[0] for v in per_kernel.values()) or 1.0
-    for name, (ms, n) in sorted(per_kernel.items(), key=lambda kv: -kv[1][0]):
-        kernels.append({"name": name, "launches_per_step": n / args.steps, "ms_per_launch": ms / n,
-                        "share": ms / kern_total})
+    kernels = [{"name": k, "launches_per_step": n / args.steps, "ms_per_launch": ms / n, "share": ms / kern_total}
+               for k, (ms, n) in sorted(per_kernel.items(), key=lambda kv: -kv[1][0])]
     roofline = {
         "bound": "hbm",
         "achieved": achieved,
@@ -263,33 +465,33 @@ def run_ours(args) -> None:
         "unit": "GB/s",
         "frac": achieved / peak,
         "traffic": None,
-        "peak_kind": f"{peak_kind} hbm_gbs",
-        "scope": "fused sweep (all passes of one sweep, CUDA events on its stream)",
+        "peak_kind": f"{peak_kind} hbm_gbs (of {peak_kind})",
+        "scope": "fused sweep: all passes of one sweep on one stream, algorithmic bytes per sweep / sweep time",
         "algorithmic_bytes_per_sweep": sweep_bytes,
-        "profiled_sweep_ms": sweep_ms,
+        "profiled_sweep_ms": statistics.median(prof_ms),
         "kernels": kernels,
     }
 
     # ---- e2e: public API with pinned host buffers -----------------------------------
     host = prob["host"]
-    hs = torch.from_numpy(host["sample"]).pin_memory()
-    hp = torch.from_numpy(host["probe"]).pin_memory()
-    hpos = torch.from_numpy(host["positions"]).pin_memory()
-    out_gs = torch.empty_like(hs).pin_memory()
-    out_gp = torch.empty_like(hp).pin_memory()
+    h_obj = torch.from_numpy(host["obj"]).pin_memory()
+    h_aux = torch.from_numpy(host["aux"]).pin_memory()
+    h_pos = torch.from_numpy(host["pos"]).pin_memory()
+    out_go = torch.empty_like(h_obj).pin_memory()
+    out_ga = torch.empty_like(h_aux).pin_memory()
     out_loss = torch.empty((), dtype=torch.float64).pin_memory()
 
     def e2e_step():
-        ds = hs.to(dev, non_blocking=True).requires_grad_(True)
-        dp = hp.to(dev, non_blocking=True).requires_grad_(True)
-        dpos = hpos.to(dev, non_blocking=True)
-        loss = ptychoX_base_loss(ds, dp, dpos, meas, scale)
+        d_obj = h_obj.to(dev, non_blocking=True).requires_grad_(True)
+        d_aux = h_aux.to(dev, non_blocking=True).requires_grad_(True)
+        d_pos = h_pos.to(dev, non_blocking=True)
+        loss = wl.loss_api(d_obj, d_aux, d_pos, prob)
         loss.backward()
         if world > 1:
-            dist.all_reduce(ds.grad)
-            dist.all_reduce(dp.grad)
-        out_gs.copy_(ds.grad, non_blocking=True)
-        out_gp.copy_(dp.grad, non_blocking=True)
+            dist.all_reduce(d_obj.grad)
+            dist.all_reduce(d_aux.grad)
+        out_go.copy_(d_obj.grad, non_blocking=True)
+        out_ga.copy_(d_aux.grad, non_blocking=True)
         out_loss.copy_(loss.detach(), non_blocking=True)
 
     for _ in range(max(1, args.warmup)):
@@ -297,27 +499,26 @@ def run_ours(args) -> None:
     torch.cuda.synchronize(dev)
     if world > 1:
         dist.barrier()
-    e2e_ms = sum(timed(args.steps, e2e_step))
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    h2d = hs.numel() * 8 + hp.numel() * 8 + hpos.numel() * 8
-    d2h = out_gs.numel() * 8 + out_gp.numel() * 8 + 8
+    e2e_ms = max_over_ranks(sum(timed(args.steps, e2e_step)))
+    h2d = (h_obj.numel() + h_aux.numel()) * 8 + h_pos.numel() * h_pos.element_size()
+    d2h = (out_go.numel() + out_ga.numel()) * 8 + 8
     e2e = {"value": world * args.steps / (e2e_ms / 1e3), "unit": "sweeps/s", "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h,
-           "note": "measured counts resident in HBM (uploaded once, as in the reference training loop); "
-                   "object, probe, positions uploaded and loss + gradients read back every step"}
+           "note": "measured counts resident in HBM (uploaded once, as the reference training loop keeps "
+                   "observed amplitudes on the device); object, probe/pupil/mask and positions uploaded and "
+                   "the loss and both gradients read back every step"}
 
     # ---- CPU baseline (rank 0, N = 1) --------------------------------------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_sample_rate(host, meas.cpu().numpy(), scale, budget_s=args.cpu_budget)
+        cpu = cpu_sample_rate(wl, host, prob["meas"].cpu().numpy(), prob["scale"], budget_s=args.cpu_budget)
 
     if rank == 0:
-        n_obj, p = prob["n_obj"], ph
+        cfg = wl.config()
+        cfg["parallelism"] = f"dp{world} (per-rank positions, NCCL all-reduce of gradients)" if world > 1 else "single GPU"
+        cfg["l2"] = "flushed between timed steps (256 MB write outside the step events)"
         line = {
-            "metric": f"fwd+adj sweeps/s ({batch}×{p}²→{n_obj}²)",
+            "metric": wl.metric(),
             "value": value,
             "unit": "sweeps/s",
             "n_gpus": world,
@@ -328,15 +529,8 @@ def run_ours(args) -> None:
             "scaling": "weak",
             "vs_baseline": None,
             "dtype": "c64 (FP32 FFT/constraint, FP64 loss sum)",
-            "data": "synthetic (seeded object/probe/raster, Poisson uint16 counts)",
-            "config": {
-                "workload": args.workload,
-                "positions": batch,
-                "probe": [p, p],
-                "object": [n_obj, n_obj],
-                "parallelism": f"dp{world}" if world > 1 else "single GPU",
-                "l2": "flushed between timed steps (256 MB write outside the step events)",
-            },
+            "data": "synthetic (seeded object and scan, Poisson uint16 counts from the forward model)",
+            "config": cfg,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
@@ -349,27 +543,26 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
-def cpu_sample_rate(host, measured, scale, budget_s: float = 12.0) -> dict:
-    """Time the CPU oracle (complex64, all host threads) on a bounded sample of positions."""
+def cpu_sample_rate(wl, host, measured, scale, budget_s: float = 12.0) -> dict:
+    """Time the CPU oracle (complex64, all host threads) on a bounded sample of the units."""
     from oracle import ptycho_oracle as O
 
     workers = O.default_workers()
-    pos = host["positions"]
-    batch = len(pos)
+    batch = wl.batch
 
     def run(k):
         t0 = time.perf_counter()
-        O.base_sweep(host["sample"], host["probe"], pos[:k], measured[:k], scale, fp64=False, workers=workers)
+        wl.cpu_sweep(host, measured, scale, k, workers)
         return time.perf_counter() - t0
 
-    k = min(batch, 16)
+    k = min(batch, 4)
+    run(k)  # warm-up (FFT plans, page faults)
     t = run(k)
-    per_pos = t / k
-    k2 = int(max(k, min(batch, budget_s / max(per_pos, 1e-6))))
+    k2 = int(max(k, min(batch, budget_s / max(t / k, 1e-6))))
     t2 = run(k2)
     sweeps_per_s = (k2 / batch) / t2
     return {"value": sweeps_per_s, "unit": "sweeps/s", "cores": workers, "kind": "port",
-            "sample": f"{k2} of {batch} positions per timed run, scaled to one sweep; complex64 numpy/scipy "
+            "sample": f"{k2} of {batch} {wl.units} per timed run, scaled to one sweep; complex64 numpy/scipy "
                       f"restatement of the reference torch CPU path ({t2:.1f} s)"}
 
 
@@ -383,28 +576,39 @@ def run_reference(args) -> None:
     if rank != 0:
         return
     from oracle import ptycho_oracle as O
-    from ptychox_b200 import synth
 
-    n_obj, p, grid, step_px, origin, jitter, photons = WORKLOADS[args.workload]
-    rng = np.random.default_rng(1000)
-    obj = synth.random_object(n_obj, n_obj, rng)
-    probe = synth.gaussian_probe(p, p, rng)
-    pos = synth.raster_positions(grid, step_px, origin, jitter, rng)
-    batch = len(pos)
+    wl = WORKLOADS[args.workload]
     workers = O.default_workers()
-    # a bounded sample per step: enough positions for ~2 s of work
-    k = min(batch, 8)
-    amp, _, _ = O.base_forward(obj, probe, pos[:k], fp64=False, workers=workers)
+    h = wl.host(1000)
+    batch = wl.batch
+    # a bounded sample per step: enough units for ~2 s of work; counts from the oracle forward
+    rng = np.random.default_rng(7)
+
+    def counts(k):
+        if isinstance(wl, Coded):
+            _, _, _, amp = O.coded_forward(h["truth"], h["aux"], h["t1"], h["t2"], h["pos"][:k], wl.ds, fp64=False,
+                                           workers=workers)
+        elif isinstance(wl, Fourier):
+            amp, _, _ = O.fpm_forward(h["truth"], h["aux"], h["pos"][:k], fp64=False, workers=workers)
+        else:
+            amp, _, _ = O.base_forward(h["truth"], h["aux"], h["pos"][:k], fp64=False, workers=workers)
+        from ptychox_b200 import synth
+
+        return synth.poisson_counts(amp.astype(np.float64) ** 2, wl.photons, rng,
+                                    per_pixel=isinstance(wl, (Fourier, Coded)),
+                                    brightest=isinstance(wl, Fourier))
+
+    k = min(batch, 2)
+    meas, scale = counts(k)
+    wl.cpu_sweep(h, meas, scale, k, workers)
     t0 = time.perf_counter()
-    O.base_forward(obj, probe, pos[:k], fp64=False, workers=workers)
-    per_pos = (time.perf_counter() - t0) / k * 3.0
-    sample = int(min(batch, max(k, 2.0 / max(per_pos, 1e-6))))
-    amp, _, _ = O.base_forward(obj, probe, pos[:sample], fp64=False, workers=workers)
-    meas, scale = synth.poisson_counts(amp.astype(np.float64) ** 2, photons, rng)
-    guess = (obj * (1 + 0.1 * rng.standard_normal(obj.shape))).astype(np.complex64)
+    wl.cpu_sweep(h, meas, scale, k, workers)
+    per_unit = (time.perf_counter() - t0) / k
+    sample = int(min(batch, max(k, 2.0 / max(per_unit, 1e-6))))
+    meas, scale = counts(sample)
 
     def one():
-        O.base_sweep(guess, probe, pos[:sample], meas, scale, fp64=False, workers=workers)
+        wl.cpu_sweep(h, meas, scale, sample, workers)
 
     for _ in range(args.warmup):
         one()
@@ -417,7 +621,7 @@ def run_reference(args) -> None:
     value = 1.0 / per_sweep
     line = {
         "impl": "reference",
-        "metric": f"fwd+adj sweeps/s ({batch}×{p}²→{n_obj}²)",
+        "metric": wl.metric(),
         "value": value,
         "unit": "sweeps/s",
         "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
@@ -429,9 +633,10 @@ def run_reference(args) -> None:
         "vs_baseline": None,
         "dtype": "c64",
         "data": "synthetic (seeded)",
-        "config": {"workload": args.workload, "positions": batch, "probe": [p, p], "object": [n_obj, n_obj]},
+        "config": wl.config(),
         "cpu_baseline": {"value": value, "unit": "sweeps/s", "cores": workers, "kind": "port",
-                         "sample": f"{sample} of {batch} positions per step, scaled to one sweep"},
+                         "sample": f"{sample} of {batch} {wl.units} per step, scaled to one sweep; complex64 "
+                                   "numpy/scipy restatement of the reference torch CPU path"},
         "e2e": {"value": value, "unit": "sweeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
