@@ -395,12 +395,12 @@ def run_ours(args) -> None:
     ws = wl.workspace(prob, dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
+    from ptychox_b200.distributed import reduce_sweep
+
     def step():
         loss, g_obj, g_aux = wl.sweep(prob, ws)
-        if world > 1:  # data-parallel sweep: sum the ranks' gradients
-            dist.all_reduce(g_obj)
-            dist.all_reduce(g_aux)
-            dist.all_reduce(loss)
+        if world > 1:  # data-parallel sweep: global mean over all ranks' units
+            reduce_sweep(loss, [g_obj, g_aux], wl.batch, wl.batch * world)
         return loss
 
     def timed(k: int, fn) -> list[float]:
@@ -488,8 +488,7 @@ def run_ours(args) -> None:
         loss = wl.loss_api(d_obj, d_aux, d_pos, prob)
         loss.backward()
         if world > 1:
-            dist.all_reduce(d_obj.grad)
-            dist.all_reduce(d_aux.grad)
+            reduce_sweep(loss.detach(), [d_obj.grad, d_aux.grad], wl.batch, wl.batch * world)
         out_go.copy_(d_obj.grad, non_blocking=True)
         out_ga.copy_(d_aux.grad, non_blocking=True)
         out_loss.copy_(loss.detach(), non_blocking=True)

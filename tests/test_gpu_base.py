@@ -174,3 +174,77 @@ def test_config1_subset_vs_oracle():
     assert abs(loss - rl) <= TOL * abs(rl)
     assert rel_l2(gs, rs) < TOL
     assert rel_l2(gp, rp) < TOL
+
+
+def _fd_base(obj, probe, pos, meas, scale, obj_pix, probe_pix, delta=1e-5):
+    """Central differences of the FP64 loss at single object / probe pixels.
+
+    A pixel perturbation changes each affected exit wave at one point, so the far field
+    changes by delta * value * (outer product of two DFT rows): the loss differences are
+    evaluated exactly from the stored FP64 far fields, stably as
+    (|F+D| - |F|)(|F+D| + |F| - 2Y) with |F+D| - |F| = (2 Re(conj(F) D) + |D|^2)/(|F+D| + |F|).
+    Returns (dL/dRe, dL/dIm) per pixel.
+    """
+    p = probe.shape[0]
+    obj = obj.astype(np.complex128)
+    probe = probe.astype(np.complex128)
+    _, far, _ = O.base_forward(obj, probe, pos)
+    y = O.measured_amplitude(meas, scale).astype(np.float64)
+    a = np.abs(far)
+    numel = far.size
+    k = np.arange(p) - p // 2
+
+    def dloss(b, ly, lx, d):
+        ey = np.exp(-2j * np.pi * k * ly / p)
+        ex = np.exp(-2j * np.pi * k * lx / p)
+        dF = d * np.outer(ey, ex)
+        F = far[b]
+        anew = np.abs(F + dF)
+        diff = (2 * (np.conj(F) * dF).real + np.abs(dF) ** 2) / (anew + a[b] + 1e-300)
+        return float(np.sum(diff * (anew + a[b] - 2 * y[b]))) / numel
+
+    def central(terms):
+        out = []
+        for e in (1.0, 1j):
+            plus = sum(dloss(b, ly, lx, delta * e * v) for b, ly, lx, v in terms)
+            minus = sum(dloss(b, ly, lx, -delta * e * v) for b, ly, lx, v in terms)
+            out.append((plus - minus) / (2 * delta))
+        return out
+
+    fd_obj, fd_probe = [], []
+    for (yy, xx) in obj_pix:
+        terms = [(b, yy - y0, xx - x0, probe[yy - y0, xx - x0]) for b, (x0, y0) in enumerate(pos.tolist())
+                 if x0 <= xx < x0 + p and y0 <= yy < y0 + p]
+        fd_obj.append(central(terms))
+    for (ly, lx) in probe_pix:
+        terms = [(b, ly, lx, obj[y0 + ly, x0 + lx]) for b, (x0, y0) in enumerate(pos.tolist())]
+        fd_probe.append(central(terms))
+    return np.array(fd_obj), np.array(fd_probe)
+
+
+def test_config1_finite_differences():
+    """Config 1 frames (2048^2 object, 512^2 probe, 48-position subset): the autograd.Function
+    gradient of the fused loss vs FP64 central differences at 64 random object pixels and
+    16 random probe pixels."""
+    from ptychox_b200 import ptychoX_base_loss, synth
+
+    rng = np.random.default_rng(31)
+    obj = synth.random_object(2048, 2048, rng)
+    probe = synth.gaussian_probe(512, 512, rng)
+    pos = synth.raster_positions(30, 48, 64, 3, rng)
+    sub = pos[rng.choice(len(pos), 48, replace=False)]
+    amp, _, _ = O.base_forward(obj, probe, sub, fp64=False)
+    meas, scale = synth.poisson_counts(amp.astype(np.float64) ** 2, 1e5, rng)
+    guess = (obj * (1 + 0.1 * rng.standard_normal(obj.shape))).astype(np.complex64)
+    s = cuda(guess).requires_grad_(True)
+    p = cuda(probe).requires_grad_(True)
+    ptychoX_base_loss(s, p, cuda(sub), cuda(meas), scale).backward()
+    gs, gp = s.grad.cpu().numpy(), p.grad.cpu().numpy()
+    covered = [(int(y0 + rng.integers(0, 512)), int(x0 + rng.integers(0, 512)))
+               for x0, y0 in sub[rng.choice(len(sub), 64)].tolist()]
+    ppix = [(int(a), int(b)) for a, b in rng.integers(150, 362, size=(16, 2))]  # inside the probe's support
+    fd_o, fd_p = _fd_base(guess, probe, sub, meas, scale, covered, ppix)
+    g_o = np.array([[gs[y, x].real, gs[y, x].imag] for y, x in covered])
+    g_p = np.array([[gp[a, b].real, gp[a, b].imag] for a, b in ppix])
+    assert rel_l2(g_o, fd_o) < TOL
+    assert rel_l2(g_p, fd_p) < TOL
