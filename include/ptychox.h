@@ -192,6 +192,24 @@ int ptx_coded_sweep(const float* object, const float* coded_surface,
                     double* loss, float* grad_object, float* grad_coded,
                     void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- optimiser step -------------------------------------------------------------
+ * Adam on a complex64 parameter with torch.optim.Adam semantics (the reference drivers'
+ * optimiser, python/train_ptychography.py:500-507): the (re, im) pairs are independent
+ * reals, m = lerp(m, g, 1-b1), v = b2 v + (1-b2) g^2,
+ * p -= lr/(1-b1^t) * m / (sqrt(v)/sqrt(1-b2^t) + eps); then an optional projection:
+ * PTX_CONSTRAIN_UNIT_AMPLITUDE (|z| <= 1, phase kept; the MATLAB scripts' object clamp)
+ * or PTX_CONSTRAIN_REAL_NONNEGATIVE (z -> max(Re z, 0); train_coded.py:242-244).
+ * `state` is 16 bytes of device memory, zeroed before the first step; it holds the step
+ * count, so the call can be captured in a CUDA graph and replayed.  exp_avg and
+ * exp_avg_sq are complex64-shaped (n_complex pairs) and zero at the start.  All four
+ * arrays must be 16-byte aligned. */
+#define PTX_CONSTRAIN_NONE 0
+#define PTX_CONSTRAIN_UNIT_AMPLITUDE 1
+#define PTX_CONSTRAIN_REAL_NONNEGATIVE 2
+int ptx_adam_step(float* param, const float* grad, float* exp_avg, float* exp_avg_sq,
+                  size_t n_complex, void* state, float lr, float beta1, float beta2, float eps,
+                  int constraint, void* stream);
+
 /* Allocation-free fused sweep, for callers that cannot allocate device memory: a host
  * program that loads this library as a plug-in and keeps the GPU memory pool to itself,
  * or an acquisition loop that must not take the device-wide synchronisation of a

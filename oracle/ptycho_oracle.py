@@ -60,6 +60,7 @@ __all__ = [
     "coded_sweep",
     "nearfield_sweep",
     "default_workers",
+    "adam_step",
 ]
 
 
@@ -351,3 +352,39 @@ def nearfield_sweep(object_field, probe_field, transfer, shifts_xy, downsample, 
     """Near-field = coded with ``transfer_1 = 1`` (``adPtychoX_nearf.m:44-62``)."""
     return coded_sweep(object_field, probe_field, None, transfer, shifts_xy, downsample,
                        measured_u16, scale, fp64, workers)
+
+
+# ----------------------------------------------------------------------------------------
+# Optimiser step
+# ----------------------------------------------------------------------------------------
+
+
+def adam_step(param, grad, exp_avg, exp_avg_sq, step, lr, beta1=0.9, beta2=0.999, eps=1e-16,
+              constraint=None):
+    """One Adam step on a complex parameter, as torch.optim.Adam does it (torch/optim/adam.py,
+    single-tensor path): complex values are (re, im) pairs of independent reals.
+
+    Used by ``train_ptychography.py:500-507`` (betas (0.9, 0.999), eps 1e-16).  Optional
+    projection afterwards: ``"unit_amplitude"`` (|z| <= 1, phase kept) or
+    ``"real_nonnegative"`` (z -> max(Re z, 0), ``train_coded.py:242-244``).
+    Returns new ``(param, exp_avg, exp_avg_sq)``; ``step`` is the 1-based step number.
+    """
+    rd = np.float32 if np.asarray(param).dtype == np.complex64 else np.float64
+    p = np.asarray(param).view(rd).copy()
+    g = np.asarray(grad).astype(param.dtype).view(rd)
+    m = np.asarray(exp_avg).view(rd).copy()
+    v = np.asarray(exp_avg_sq).view(rd).copy()
+    m = m + rd(1 - beta1) * (g - m)
+    v = rd(beta2) * v + rd(1 - beta2) * g * g
+    bc1 = 1 - beta1 ** step
+    bc2 = 1 - beta2 ** step
+    step_size = rd(lr / bc1)
+    denom = np.sqrt(v) / rd(bc2 ** 0.5) + rd(eps)
+    p = p - step_size * (m / denom)
+    z = p.view(np.asarray(param).dtype)
+    if constraint == "unit_amplitude":
+        a = np.abs(z)
+        z = np.where(a > 1, z / np.maximum(a, 1e-30), z)
+    elif constraint == "real_nonnegative":
+        z = np.maximum(z.real, 0).astype(z.dtype)
+    return z.astype(np.asarray(param).dtype), m.view(np.asarray(param).dtype), v.view(np.asarray(param).dtype)

@@ -20,6 +20,10 @@ PTX_ERR_CUDA = 4
 PTX_ERR_OUT_OF_BOUNDS = 5
 PTX_ERR_TIMEOUT = 6
 
+PTX_CONSTRAIN_NONE = 0
+PTX_CONSTRAIN_UNIT_AMPLITUDE = 1
+PTX_CONSTRAIN_REAL_NONNEGATIVE = 2
+
 _p = C.c_void_p
 _i = C.c_int
 _f = C.c_float
@@ -50,6 +54,7 @@ SIGNATURES: dict[str, tuple] = {
     "ptx_coded_forward": (_i, [_p, _p, _p, _p, _i, _p, _i, _i, _p, _p, _p, _p, _sz, _p]),
     "ptx_coded_backward": (_i, [_p, _p, _p, _p, _p, _p, _p, _i, _p, _i, _i, _p, _p, _p, _sz, _p]),
     "ptx_coded_sweep": (_i, [_p, _p, _p, _p, _i, _p, _i, _i, _p, _f, _p, _p, _p, _p, _sz, _p]),
+    "ptx_adam_step": (_i, [_p, _p, _p, _p, _sz, _p, _f, _f, _f, _f, _i, _p]),
     "ptx_base_sweep_noalloc": (_i, [_p, _i, _i, _p, _i, _i, _p, _i, _p, _f, _p, _p, _p, _p]),
 }
 

@@ -1,0 +1,59 @@
+"""Serving: each reconstruction's result is the same alone and in the mixed stream.
+
+Tolerance: relative L2 1e-4 on the final object and probe / pupil / mask, 1e-4 on the
+final loss -- float atomics make runs differ at the 1e-7 level per sweep, and 12 Adam
+iterations carry those differences forward.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def small_mix():
+    from ptychox_b200.serving import synthesize_request
+
+    specs = [
+        (0, "conventional", {"p": 64, "grid": 5, "step": 16, "n": 160}),
+        (1, "fourier", {"n": 128, "h": 32, "grid": 5}),
+        (2, "coded", {"n": 64, "count": 6, "ds": 2}),
+        (3, "conventional", {"p": 96, "grid": 4, "step": 24, "n": 208}),  # runtime-plan length
+        (4, "nearfield", {"n": 64, "count": 5, "ds": 4}),
+        (5, "fourier", {"n": 64, "h": 16, "grid": 3}),
+    ]
+    return [synthesize_request(rid, m, 0.0, size, seed=100 + rid, device="cuda", iters=12) for rid, m, size in specs]
+
+
+def test_alone_equals_mixed_and_plain():
+    from ptychox_b200.serving import ReconstructionServer, run_plain
+
+    reqs = small_mix()
+    mixed = ReconstructionServer("cuda", max_active=8).run(reqs, realtime=False)
+    for req, res in zip(reqs, mixed):
+        alone = ReconstructionServer("cuda").run([req], realtime=False)[0]
+        assert res.rid == alone.rid == req.rid
+        assert np.isfinite(res.final_loss)
+        assert abs(res.final_loss - alone.final_loss) <= 1e-4 * abs(alone.final_loss)
+        assert rel_l2(res.obj, alone.obj) < 1e-4
+        assert rel_l2(res.aux, alone.aux) < 1e-4
+    plain = run_plain(reqs, "cuda", realtime=False)
+    for res, pl in zip(mixed, plain):
+        # same math through the unfused operators and torch.optim.Adam
+        assert abs(res.final_loss - pl.final_loss) <= 1e-3 * abs(pl.final_loss)
+        assert rel_l2(res.obj, pl.obj) < 1e-3
+
+
+def test_budget_admission_and_no_graph_path():
+    from ptychox_b200.serving import ReconstructionServer, request_bytes
+
+    reqs = small_mix()[:3]
+    need = max(request_bytes(r, 512 << 20) for r in reqs)
+    # a budget that holds one reconstruction at a time still serves all of them
+    res = ReconstructionServer("cuda", hbm_budget=need, use_graphs=False).run(reqs, realtime=False)
+    assert [r.rid for r in res] == [0, 1, 2] and all(np.isfinite(r.final_loss) for r in res)
+    with pytest.raises(ValueError):
+        ReconstructionServer("cuda", hbm_budget=need // 4).run(reqs, realtime=False)
