@@ -679,7 +679,7 @@ def run_serving(args) -> None:
     clocks.start()
     launches0 = _abi.query("ptx_launch_count")
     t0 = time.perf_counter()
-    served = ReconstructionServer(dev).run(reqs, realtime=True)
+    served = ReconstructionServer(dev, max_active=args.max_active).run(reqs, realtime=True)
     t_served = time.perf_counter() - t0
     launches = _abi.query("ptx_launch_count") - launches0
     clk = clocks.stop()
@@ -708,6 +708,7 @@ def run_serving(args) -> None:
         "dtype": "c64 (FP32 FFT/constraint, FP64 loss sum)",
         "data": "synthetic (seeded problems, Poisson uint16 counts from the forward model)",
         "config": {"workload": "serving-mix", "requests": len(reqs), "arrival_rate_per_s": 20.0,
+                   "max_active": args.max_active,
                    "iterations_per_request": args.iters, "mix": by_mod,
                    "mix_rule": "40/30/20/10% configs 0/2/3/1, sizes x U[0.75,1.25]"},
         "served": {"wall_s": t_served, "sweeps_per_s": sweeps / t_served, "p50_latency_s": percentile(lat_s, 50),
@@ -731,6 +732,7 @@ def main() -> None:
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS) + ["serving-mix"])
     ap.add_argument("--requests", type=int, default=40)
     ap.add_argument("--iters", type=int, default=50)
+    ap.add_argument("--max-active", type=int, default=8)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=12.0)

@@ -121,10 +121,10 @@ def request_bytes(req: ReconRequest, ws_cap: int) -> int:
 class _Slot:
     """Resident state of one admitted reconstruction and its captured iteration."""
 
-    def __init__(self, req: ReconRequest, dev: torch.device, ws_cap: int, use_graph: bool):
+    def __init__(self, req: ReconRequest, dev: torch.device, ws_cap: int, use_graph: bool, priority: int = 0):
         self.req = req
         self.dev = dev
-        self.stream = torch.cuda.Stream(device=dev)
+        self.stream = torch.cuda.Stream(device=dev, priority=priority)
         self.iters_launched = 0
         self.bytes = request_bytes(req, ws_cap)
         with torch.cuda.stream(self.stream):
@@ -204,7 +204,7 @@ class ReconstructionServer:
     """Admit by HBM budget, keep state resident, replay captured iterations concurrently."""
 
     def __init__(self, device: torch.device | str = "cuda", hbm_budget: int | None = None,
-                 max_active: int = 32, workspace_cap: int = 512 << 20, use_graphs: bool = True,
+                 max_active: int = 8, workspace_cap: int = 512 << 20, use_graphs: bool = True,
                  max_inflight: int = 2):
         self.dev = torch.device(device)
         if hbm_budget is None:
@@ -237,7 +237,10 @@ class ReconstructionServer:
                 if used + need > self.budget and active:
                     break
                 pending.pop(0)
-                slot = _Slot(nxt, self.dev, self.ws_cap, self.use_graphs)
+                # older reconstructions get higher stream priority (the GPU prefers their CTAs)
+                low, high = torch.cuda.Stream.priority_range()
+                prio = max(high, min(low, high + len(active)))
+                slot = _Slot(nxt, self.dev, self.ws_cap, self.use_graphs, priority=prio)
                 used += slot.bytes
                 active.append(slot)
                 results[nxt.rid].admitted = clock() if realtime else 0.0
@@ -333,6 +336,11 @@ def snap_smooth(n: float) -> int:
     return min(_SMOOTH, key=lambda m: (abs(m - n), m))
 
 
+def snap_pow2(n: float) -> int:
+    """Nearest power-of-two transform length in [16, 1024] (ties round up)."""
+    return min((2 ** a for a in range(4, 11)), key=lambda m: (abs(math.log2(m) - math.log2(n)), -m))
+
+
 def synthesize_request(rid: int, modality: str, arrival: float, size: dict, seed: int, device,
                        iters: int = 50) -> ReconRequest:
     """One seeded reconstruction problem; counts from the forward model of the truth.
@@ -401,8 +409,10 @@ def serving_mix(n_requests: int, seed: int = 0, rate: float = 20.0) -> list[tupl
     conventional small scan (128^2 probe, 11x11 raster), Fourier (256^2 pupil, 15x15
     LEDs, 1024^2 spectrum), coded / near-field (1024^2 field, 64 shifts, ds 4) and the
     conventional large scan (512^2 probe, 30x30 raster); sizes jittered by U[0.75, 1.25]
-    and snapped to supported lengths (probes to 2^a 3^b 5^c, positions capped at 900 and
-    floored at 49; Fourier and coded sides stay powers of two).
+    and snapped to the lengths of the register-FFT kernels: probe sides to the nearest
+    power of two (other 2^a 3^b 5^c lengths run on the slower runtime-plan kernels), scan
+    grids jittered with positions capped at 900 and floored at 49, Fourier and coded sides
+    kept (powers of two).
     """
     rng = np.random.default_rng(seed)
     t = 0.0
@@ -414,7 +424,7 @@ def serving_mix(n_requests: int, seed: int = 0, rate: float = 20.0) -> list[tupl
         if u < 0.4 or u >= 0.9:
             big = u >= 0.9
             p0, g0, s0 = (512, 30, 48) if big else (128, 11, 32)
-            p = snap_smooth(p0 * j())
+            p = snap_pow2(p0 * j())
             grid = int(min(30, max(7, round(g0 * j()))))
             step = max(4, int(round(s0 * p / p0)))
             n = 8 + (grid - 1) * step + p + 4 + 8
