@@ -217,8 +217,9 @@ int ptx_adam_step(float* param, const float* grad, float* exp_avg, float* exp_av
  * temporary with torch::empty / torch::zeros, base_kernel.cu:250-251,281-282).
  * Same arguments and results as ptx_base_sweep minus the workspace: the scratch frames
  * live in a fixed PTX_NOALLOC_SCRATCH_BYTES device array that every GPU loading the
- * library holds until exit.  A probe frame (width rounded up to 16) times 8 bytes plus
- * 256 must fit in it, else PTX_ERR_WORKSPACE.  The first call on a device looks up the
+ * library holds until exit.  ptx_base_workspace_bytes(probe_h, probe_w, 1) (one frame of
+ * ph x pw rounded up to 16 columns, 8 bytes each, plus a 256 KiB table and 256 bytes)
+ * must fit in it, else PTX_ERR_WORKSPACE.  The first call on a device looks up the
  * array's device address (make it before any CUDA graph capture).  All calls share the
  * array: calls that overlap on the GPU race and must be serialised by the caller. */
 #define PTX_NOALLOC_SCRATCH_BYTES (8u * 1024u * 1024u)

@@ -20,12 +20,12 @@
 #include <cstdlib>
 
 #include "ptx_internal.h"
-#include "ptx_regfft.cuh"
+#include "ptx_passes.cuh"
 
 namespace ptx {
 namespace {
 
-constexpr size_t kHeaderBytes = 256;           // error word + padding
+constexpr size_t kHeaderBytes = 256 + kLutBytes;  // error word + padding, count-decode table
 constexpr size_t kTargetScratch = 4096ull << 20;  // upper bound on workspace frames
 constexpr float kEps = 1.1920928955078125e-07f;  // torch.finfo(float32).eps
 
@@ -317,7 +317,7 @@ struct ColCfg {
 template <int MODE, int N>
 __global__ void __launch_bounds__(256, 2) base_cols_reg(
     float2* __restrict__ scratch, int pw, int frame0, const float2* __restrict__ tw,
-    const uint16_t* __restrict__ measured, float scale, float grad_scale, double inv_numel,
+    const uint16_t* __restrict__ measured, const float* __restrict__ lut, float grad_scale, double inv_numel,
     double* __restrict__ loss, float2* __restrict__ far_field, float* __restrict__ amplitude,
     const float* __restrict__ grad_output) {
   using S = RegShape<N>;
@@ -375,21 +375,23 @@ __global__ void __launch_bounds__(256, 2) base_cols_reg(
   if (MODE == kColSweep) {
     cp_async_wait_all();
     __syncthreads();
-    double acc = 0.0;
+    float part = 0.f;  // this thread's N1 squared residuals; summed in FP64 across the grid
 #pragma unroll
     for (int m = 0; m < S::N1; ++m) {
       const int kr = t + S::T * m;
       const float2 F = v[m];
       float2 out = make_float2(0.f, 0.f);
       if (col_ok) {
-        const float y = sqrtf(static_cast<float>(meas_s[kr * kColsReg + c]) * scale);
-        const float a = cabsf(F);
+        const float y = __ldg(&lut[meas_s[kr * kColsReg + c]]);
+        float a, inv;
+        abs_and_inv(F, kEps, a, inv);
         const float rr = a - y;
-        acc += static_cast<double>(rr) * static_cast<double>(rr);
-        out = cscale(F, grad_scale * rr / fmaxf(a, kEps));
+        part = fmaf(rr, rr, part);
+        out = cscale(F, grad_scale * rr * inv);
       }
       v[m] = out;
     }
+    double acc = static_cast<double>(part);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if ((tid & 31) == 0) red[tid >> 5] = acc;
@@ -451,14 +453,29 @@ __global__ void __launch_bounds__(128, 3) base_rows_adjoint_reg(
   const bool row_ok = r < ph;
   const int f0 = blockIdx.y * frames_per_cta;
   const int f1 = min(nframes, f0 + frames_per_cta);
-  float2* buf = sm + l * RowCfg<N>::LP;
+  // line buffer: the FFT's exchange buffer, and between transforms the landing place of
+  // the next frame's scratch row (prefetched with cp.async while this frame scatters)
+  constexpr int BP = RowCfg<N>::LP > N ? RowCfg<N>::LP : N;
+  float2* buf = sm + l * BP;
   // this line's object row, prefetched with cp.async (each thread copies and later reads
   // exactly the elements it owns, so only its own copies need waiting for)
-  float2* obuf = sm + lines * RowCfg<N>::LP + l * N;
+  float2* obuf = sm + lines * BP + l * N;
   const float2* prow = probe + (size_t)(row_ok ? r : 0) * N;
   float2 acc[S::N1];
 #pragma unroll
   for (int m = 0; m < S::N1; ++m) acc[m] = make_float2(0.f, 0.f);
+  // thread t copies / reads the scratch elements c = t + T j of its row (same ownership
+  // as the FFT input), so each thread only waits for its own copies
+  auto prefetch_row = [&](int f) {
+    const float2* base = scratch + (size_t)f * kTiles * ph * kTile + (size_t)r * kTile;
+#pragma unroll
+    for (int j = 0; j < S::N1; ++j) {
+      const int c = t + S::T * j;
+      cp_async8(buf + c, base + (size_t)(c / kTile) * ph * kTile + (c % kTile));
+    }
+    cp_async_commit();
+  };
+  if (row_ok && f0 < f1) prefetch_row(f0);
   for (int f = f0; f < f1; ++f) {
     const long long x0 = pos[2 * f], y0 = pos[2 * f + 1];
     const bool ok = window_ok(x0, y0, ph, N, H, W);
@@ -470,20 +487,30 @@ __global__ void __launch_bounds__(128, 3) base_rows_adjoint_reg(
     }
     float2 v[S::N1];
     if (row_ok) {
-      const float2* base = scratch + (size_t)f * kTiles * ph * kTile + (size_t)r * kTile;
-#pragma unroll
-      for (int j = 0; j < S::N1; ++j) {
-        const int c = t + S::T * j;
-        v[j] = base[(size_t)(c / kTile) * ph * kTile + (c % kTile)];
+      // wait for the scratch row (committed before the object row)
+      if (ok) {
+        asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+      } else {
+        cp_async_wait_all();
       }
+#pragma unroll
+      for (int j = 0; j < S::N1; ++j) v[j] = buf[t + S::T * j];
     } else {
 #pragma unroll
       for (int j = 0; j < S::N1; ++j) v[j] = make_float2(0.f, 0.f);
     }
+    __syncwarp();
     reg_fft<N, true, false>(v, buf, t, tw);
+    const bool more = row_ok && f + 1 < f1;
+    if (more) prefetch_row(f + 1);
     if (row_ok && ok) {
       float2* grow = grad_sample + (y0 + r) * W + x0;
-      cp_async_wait_all();
+      // the object row of this frame; the next scratch row may stay in flight
+      if (more) {
+        asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+      } else {
+        cp_async_wait_all();
+      }
 #pragma unroll
       for (int m = 0; m < S::N1; ++m) {
         const int c = t + S::T * m;
@@ -510,7 +537,9 @@ struct RegLaunch {
     return l < need ? l : need;
   }
   static int row_smem(int lines) { return lines * RowCfg<N>::LP * (int)sizeof(float2); }
-  static int adj_smem(int lines) { return lines * (RowCfg<N>::LP + N) * (int)sizeof(float2); }
+  static int adj_smem(int lines) {
+    return lines * ((RowCfg<N>::LP > N ? RowCfg<N>::LP : N) + N) * (int)sizeof(float2);
+  }
   static int col_threads() { return kColsReg * T; }
   static int col_smem() { return ColCfg<N>::kSmemBytes; }
 };
@@ -523,6 +552,7 @@ struct BaseGeom {
   size_t frame_bytes;
   int chunk;
   unsigned* err;
+  float* lut;
   float2* scratch;
 };
 
@@ -554,6 +584,7 @@ int check_common(const void* sample, int H, int W, const void* probe, int ph, in
   }
   g->chunk = static_cast<int>(std::min<size_t>(fit, (size_t)std::max(batch, 1)));
   g->err = reinterpret_cast<unsigned*>(ws);
+  g->lut = reinterpret_cast<float*>(static_cast<char*>(ws) + 256);
   g->scratch = reinterpret_cast<float2*>(static_cast<char*>(ws) + kHeaderBytes);
   int st = PTX_OK;
   dispatch_len(pw, [&](auto NT) {
@@ -647,7 +678,7 @@ void launch_cols(const BaseGeom& g, int frame0, int nframes, const uint16_t* mea
       using L = RegLaunch<N>;
       dim3 grid(num_tiles(g.pw) * (kTile / kColsReg), nframes);
       base_cols_reg<MODE, N><<<grid, L::col_threads(), L::col_smem(), s>>>(
-          g.scratch, g.pw, frame0, g.col.tw, measured, scale, grad_scale, inv_numel, loss, far_field, amplitude,
+          g.scratch, g.pw, frame0, g.col.tw, measured, g.lut, grad_scale, inv_numel, loss, far_field, amplitude,
           grad_output);
     } else {
       dim3 grid(num_tiles(g.pw) * (kTile / g.cs.cols), nframes);
@@ -747,6 +778,9 @@ int ptx_base_sweep(const float* sample, int sample_h, int sample_w, const float*
   cudaMemsetAsync(g.err, 0, sizeof(unsigned), s);
   const double numel = (double)batch * probe_h * probe_w;
   const float grad_scale = static_cast<float>(2.0 / std::max(numel, 1.0));
+  prof_begin(kMiscKernel, s);
+  decode_lut_kernel<<<kLutEntries / 256, 256, 0, s>>>(g.lut, scale);
+  prof_end(kMiscKernel, s);
   const float2* S = reinterpret_cast<const float2*>(sample);
   const float2* P = reinterpret_cast<const float2*>(probe);
   for (int b0 = 0; b0 < batch; b0 += g.chunk) {

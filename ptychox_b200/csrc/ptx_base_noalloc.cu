@@ -10,8 +10,9 @@
 //
 // Limits and rules:
 //   - the array holds kNoallocScratchBytes (8 MiB) on every GPU that loads this library,
-//     until the process exits; a probe frame (rounded up to 16 columns) plus a 256-byte
-//     header must fit in it, otherwise the call returns PTX_ERR_WORKSPACE;
+//     until the process exits; one probe frame (rounded up to 16 columns) plus the
+//     256 KiB count-decode table and a 256-byte header must fit in it, otherwise the call
+//     returns PTX_ERR_WORKSPACE;
 //   - in host code the array's name is not a device address, so the first call on each
 //     device looks the address up with cudaGetSymbolAddress (with that device current)
 //     and caches it; make that first call before any CUDA graph capture;
@@ -62,12 +63,12 @@ extern "C" int ptx_base_sweep_noalloc(const float* sample, int sample_h, int sam
                                       float* grad_probe, void* stream) {
   using namespace ptx;
   if (probe_h <= 0 || probe_w <= 0) return set_error(PTX_ERR_INVALID_ARGUMENT, "non-positive probe shape");
-  const size_t frame = (size_t)num_tiles(probe_w) * kTile * probe_h * sizeof(float2);
-  if (256 + frame > kNoallocScratchBytes) {
+  const size_t need = ptx_base_workspace_bytes(probe_h, probe_w, 1);  // header, decode table, one frame
+  if (need > kNoallocScratchBytes) {
     return set_error(PTX_ERR_WORKSPACE,
                      "a %d x %d probe frame needs %zu bytes of scratch; ptx_base_sweep_noalloc has a fixed "
                      "%zu-byte scratch (use ptx_base_sweep with a caller workspace)",
-                     probe_h, probe_w, 256 + frame, kNoallocScratchBytes);
+                     probe_h, probe_w, need, kNoallocScratchBytes);
   }
   void* scratch = nullptr;
   if (int st = noalloc_scratch(&scratch)) return st;

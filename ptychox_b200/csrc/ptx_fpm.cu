@@ -26,7 +26,7 @@
 namespace ptx {
 namespace {
 
-constexpr size_t kHdr = 256;
+constexpr size_t kHdr = 256 + kLutBytes;  // padding, count-decode table
 enum FpmMode { kFpmSweep = 0, kFpmForward = 1, kFpmBackward = 2 };
 
 __device__ __forceinline__ int wrap2(long long v, int n) { return static_cast<int>(v & (long long)(n - 1)); }
@@ -68,7 +68,8 @@ __global__ void __launch_bounds__(256, 2) fpm_rows_forward(
 template <int MODE, int NH>
 __global__ void __launch_bounds__(256, 2) fpm_cols(
     float2* __restrict__ scratch, int lw, int frame0, const float2* __restrict__ tw,
-    const uint16_t* __restrict__ measured, float scale, float norm, float grad_scale, double inv_numel,
+    const uint16_t* __restrict__ measured, const float* __restrict__ lut, float norm, float grad_scale,
+    double inv_numel,
     double* __restrict__ loss, float2* __restrict__ image_out, float* __restrict__ amplitude,
     const float* __restrict__ grad_output) {
   using S = RegShape<NH>;
@@ -110,22 +111,23 @@ __global__ void __launch_bounds__(256, 2) fpm_cols(
   if (MODE == kFpmSweep) {
     cp_async_wait_all();
     __syncthreads();
-    double acc = 0.0;
+    float part = 0.f;  // this thread's squared residuals; summed in FP64 across the grid
 #pragma unroll
     for (int m = 0; m < S::N1; ++m) {
       const int kr = t + S::T * m;
       const float2 im = cscale(v[m], norm);
       float2 out = make_float2(0.f, 0.f);
       if (col_ok) {
-        const float y = sqrtf(static_cast<float>(meas_s[kr * kColsPerCta + c]) * scale);
-        const float a = cabsf(im);
+        const float y = __ldg(&lut[meas_s[kr * kColsPerCta + c]]);
+        float a, inv;
+        abs_and_inv(im, kEpsF32, a, inv);
         const float rr = a - y;
-        acc += static_cast<double>(rr) * static_cast<double>(rr);
-        out = cscale(im, grad_scale * rr / fmaxf(a, kEpsF32));
+        part = fmaf(rr, rr, part);
+        out = cscale(im, grad_scale * rr * inv);
       }
       v[m] = out;
     }
-    block_add_double(acc, inv_numel, loss);
+    block_add_double(static_cast<double>(part), inv_numel, loss);
   } else if (MODE == kFpmForward) {
     if (col_ok) {
 #pragma unroll
@@ -238,6 +240,7 @@ struct FpmGeom {
   float2* gspec;  // gradient w.r.t. the spectrum
   float2* tmp;    // tiled temporary of the 2-D passes
   float2* frames;
+  float* lut;     // count-decode table (sweep)
 };
 
 size_t fpm_fixed_bytes(int oh, int ow) {
@@ -270,6 +273,7 @@ int fpm_check(const void* object, int oh, int ow, const void* pupil, int lh, int
                      fixed + g->frame_bytes);
   }
   g->chunk = static_cast<int>(std::min<size_t>((ws_bytes - fixed) / g->frame_bytes, (size_t)std::max(batch, 1)));
+  g->lut = reinterpret_cast<float*>(static_cast<char*>(ws) + 256);
   char* p = static_cast<char*>(ws) + kHdr;
   g->spec = reinterpret_cast<float2*>(p);
   g->gspec = reinterpret_cast<float2*>(p + g->spec_bytes);
@@ -337,7 +341,7 @@ void launch_rows_forward(const FpmGeom& g, const float2* spec, const float2* pup
 }
 
 template <int MODE>
-void launch_cols(const FpmGeom& g, int frame0, int nf, const uint16_t* measured, float scale, float grad_scale,
+void launch_cols(const FpmGeom& g, int frame0, int nf, const uint16_t* measured, float grad_scale,
                  double inv_numel, double* loss, float2* image, float* amplitude, const float* grad_output,
                  cudaStream_t s) {
   const float norm = 1.0f / static_cast<float>((double)g.lh * g.lw);
@@ -346,7 +350,7 @@ void launch_cols(const FpmGeom& g, int frame0, int nf, const uint16_t* measured,
     constexpr int N = decltype(NT)::value;
     dim3 grid(num_tiles(g.lw) * (kTile / kColsPerCta), nf);
     fpm_cols<MODE, N><<<grid, ColPass<N>::kThreads, ColPass<N>::kSmemBytes, s>>>(
-        g.frames, g.lw, frame0, g.p_lh.tw, measured, scale, norm, grad_scale, inv_numel, loss, image, amplitude,
+        g.frames, g.lw, frame0, g.p_lh.tw, measured, g.lut, norm, grad_scale, inv_numel, loss, image, amplitude,
         grad_output);
   });
   prof_end(kFpmCols, s);
@@ -399,7 +403,7 @@ int ptx_fpm_forward(const float* object, int object_h, int object_w, const float
   for (int b0 = 0; b0 < batch; b0 += g.chunk) {
     const int nf = std::min(g.chunk, batch - b0);
     launch_rows_forward(g, spec, P, led_indices_xy + 2 * (size_t)b0, nf, s);
-    launch_cols<kFpmForward>(g, b0, nf, nullptr, 0.f, 0.f, 0.0, nullptr, reinterpret_cast<float2*>(image),
+    launch_cols<kFpmForward>(g, b0, nf, nullptr, 0.f, 0.0, nullptr, reinterpret_cast<float2*>(image),
                              amplitude, nullptr, s);
   }
   return cuda_status(cudaGetLastError(), "ptx_fpm_forward launch");
@@ -424,7 +428,7 @@ int ptx_fpm_backward(const float* grad_output, const float* image, const float* 
   float2* GP = reinterpret_cast<float2*>(grad_pupil);
   for (int b0 = 0; b0 < batch; b0 += g.chunk) {
     const int nf = std::min(g.chunk, batch - b0);
-    launch_cols<kFpmBackward>(g, b0, nf, nullptr, 0.f, 0.f, 0.0, nullptr,
+    launch_cols<kFpmBackward>(g, b0, nf, nullptr, 0.f, 0.0, nullptr,
                               const_cast<float2*>(reinterpret_cast<const float2*>(image)), nullptr, grad_output, s);
     launch_rows_adjoint(g, spec, P, led_indices_xy + 2 * (size_t)b0, nf, g.gspec, GP, s);
   }
@@ -451,6 +455,9 @@ int ptx_fpm_sweep(const float* object, int object_h, int object_w, const float* 
   cudaMemsetAsync(loss, 0, sizeof(double), s);
   const double numel = (double)batch * low_h * low_w;
   const float grad_scale = static_cast<float>(2.0 / std::max(numel, 1.0));
+  prof_begin(kMiscKernel, s);
+  decode_lut_kernel<<<kLutEntries / 256, 256, 0, s>>>(g.lut, scale);
+  prof_end(kMiscKernel, s);
   launch_fft2<false>(reinterpret_cast<const float2*>(object), object_h, object_w, g.spec, 1.0f, g.tmp, g.p_ow, g.p_oh,
                      s);
   const float2* P = reinterpret_cast<const float2*>(pupil);
@@ -459,7 +466,7 @@ int ptx_fpm_sweep(const float* object, int object_h, int object_w, const float* 
     const int nf = std::min(g.chunk, batch - b0);
     const int64_t* led = led_indices_xy + 2 * (size_t)b0;
     launch_rows_forward(g, g.spec, P, led, nf, s);
-    launch_cols<kFpmSweep>(g, b0, nf, measured, scale, grad_scale, 1.0 / std::max(numel, 1.0), loss, nullptr, nullptr,
+    launch_cols<kFpmSweep>(g, b0, nf, measured, grad_scale, 1.0 / std::max(numel, 1.0), loss, nullptr, nullptr,
                            nullptr, s);
     launch_rows_adjoint(g, g.spec, P, led, nf, g.gspec, GP, s);
   }

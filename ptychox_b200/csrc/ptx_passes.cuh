@@ -39,6 +39,33 @@ struct ColPass {
   static constexpr int kSmemBytes = kMeasOffsetBytes + N * kColsPerCta * (int)sizeof(uint16_t);
 };
 
+// ---- observed-amplitude decode table -------------------------------------------------
+// lut[c] = sqrtf(float(c) * scale) for every uint16 count c: built once per sweep with the
+// same two IEEE operations the per-element decode would use, then read by the epilogues
+// (a cached load instead of a square root per element).
+constexpr int kLutEntries = 65536;
+constexpr size_t kLutBytes = kLutEntries * sizeof(float);
+
+static __global__ void decode_lut_kernel(float* __restrict__ lut, float scale) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < kLutEntries) lut[c] = sqrtf(static_cast<float>(c) * scale);
+}
+
+// 1/sqrt(s), s > 0: the rsqrtf estimate refined by one Newton-Raphson step for the
+// reciprocal square root, y <- y (3 - s y^2) / 2.
+__device__ __forceinline__ float rsqrt_nr(float s) {
+  const float y = rsqrtf(s);
+  return y * fmaf(-0.5f * s, y * y, 1.5f);
+}
+
+// |z| and 1 / max(|z|, eps) from one reciprocal square root.
+__device__ __forceinline__ void abs_and_inv(float2 z, float eps, float& a, float& inv) {
+  const float s2 = cabs2(z);
+  const float r = rsqrt_nr(fmaxf(s2, 1e-37f));
+  a = s2 * r;
+  inv = (a >= eps) ? r : 1.0f / eps;
+}
+
 // Sum a per-thread FP64 partial over the block and add it (times `scale`) to *out.
 // Every thread of the block must call it; blocks smaller than a warp take the
 // shared-memory atomic route (a full-mask shuffle needs all 32 lanes).

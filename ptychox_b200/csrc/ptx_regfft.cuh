@@ -167,10 +167,12 @@ __host__ __device__ constexpr int row_line_pitch() {
   using S = RegShape<N>;
   return S::T >= 16 ? S::BUF : S::BUF + ((S::T - S::BUF % 16) + 16) % 16;
 }
-// Line-buffer pitch for kernels whose threads run column-fastest (column passes): odd.
+// Line-buffer pitch for kernels whose threads run column-fastest (column passes): a
+// half-warp holds 8 columns x 2 line threads, and with a pitch = 2 (mod 16) (in float2)
+// next to the odd row pitch their 16 accesses hit 16 distinct bank pairs.
 template <int N>
 __host__ __device__ constexpr int col_line_pitch() {
-  return RegShape<N>::BUF | 1;
+  return RegShape<N>::BUF + ((2 - RegShape<N>::BUF % 16) + 16) % 16;
 }
 
 template <bool BLOCK>

@@ -131,7 +131,8 @@ def test_chunked_workspace_matches():
     obj, probe, pos, meas, scale = small_problem(256, 64, 5, 40, 4, 2, 1e4, seed=4)
     full = base_sweep(cuda(obj), cuda(probe), cuda(pos), cuda(meas), scale)
     frame = 64 * 64 * 8
-    ws = torch.empty(256 + frame, dtype=torch.uint8, device="cuda")
+    hdr = 256 + 65536 * 4
+    ws = torch.empty(hdr + frame, dtype=torch.uint8, device="cuda")
     one = base_sweep(cuda(obj), cuda(probe), cuda(pos), cuda(meas), scale, ws=ws)
     assert abs(float(full[0]) - float(one[0])) <= 1e-12 * abs(float(full[0]))
     assert rel_l2(one[1].cpu().numpy(), full[1].cpu().numpy()) < 1e-6
