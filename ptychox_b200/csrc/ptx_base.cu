@@ -441,7 +441,7 @@ __global__ void __launch_bounds__(256, 2) base_cols_reg(
 template <int N>
 __global__ void __launch_bounds__(128, 3) base_rows_adjoint_reg(
     const float2* __restrict__ scratch, const float2* __restrict__ sample, int H, int W,
-    const float2* __restrict__ probe, int ph, const int64_t* __restrict__ pos, int nframes, int frames_per_cta,
+    const float2* __restrict__ probe, int ph, const int64_t* __restrict__ pos, int nframes, int rowgroups,
     float2* __restrict__ grad_sample, float2* __restrict__ grad_probe, const float2* __restrict__ tw, int lines) {
   using S = RegShape<N>;
   constexpr int kTiles = N / kTile;
@@ -449,25 +449,29 @@ __global__ void __launch_bounds__(128, 3) base_rows_adjoint_reg(
   const int tid = threadIdx.x;
   const int l = tid / S::T;
   const int t = tid - l * S::T;
-  const int r = blockIdx.x * lines + l;
-  const bool row_ok = r < ph;
-  const int f0 = blockIdx.y * frames_per_cta;
-  const int f1 = min(nframes, f0 + frames_per_cta);
+  // Work units are (row group, frame) pairs in row-group-major order; the grid is one wave
+  // of resident CTAs and CTA b takes the contiguous units [u0, u1), so every CTA does the
+  // same number of frame-rows and each covers at most a few row groups.
+  const long long units = (long long)rowgroups * nframes;
+  const long long u0 = units * blockIdx.x / gridDim.x;
+  const long long u1 = units * (blockIdx.x + 1) / gridDim.x;
+  if (u0 >= u1) return;
+  int g = static_cast<int>(u0 / nframes);
+  int f = static_cast<int>(u0 - (long long)g * nframes);
   // line buffer: the FFT's exchange buffer, and between transforms the landing place of
-  // the next frame's scratch row (prefetched with cp.async while this frame scatters)
+  // the next unit's scratch row (prefetched with cp.async while this unit scatters)
   constexpr int BP = RowCfg<N>::LP > N ? RowCfg<N>::LP : N;
   float2* buf = sm + l * BP;
   // this line's object row, prefetched with cp.async (each thread copies and later reads
   // exactly the elements it owns, so only its own copies need waiting for)
   float2* obuf = sm + lines * BP + l * N;
-  const float2* prow = probe + (size_t)(row_ok ? r : 0) * N;
   float2 acc[S::N1];
 #pragma unroll
   for (int m = 0; m < S::N1; ++m) acc[m] = make_float2(0.f, 0.f);
   // thread t copies / reads the scratch elements c = t + T j of its row (same ownership
   // as the FFT input), so each thread only waits for its own copies
-  auto prefetch_row = [&](int f) {
-    const float2* base = scratch + (size_t)f * kTiles * ph * kTile + (size_t)r * kTile;
+  auto prefetch_row = [&](int row, int frame) {
+    const float2* base = scratch + (size_t)frame * kTiles * ph * kTile + (size_t)row * kTile;
 #pragma unroll
     for (int j = 0; j < S::N1; ++j) {
       const int c = t + S::T * j;
@@ -475,8 +479,10 @@ __global__ void __launch_bounds__(128, 3) base_rows_adjoint_reg(
     }
     cp_async_commit();
   };
-  if (row_ok && f0 < f1) prefetch_row(f0);
-  for (int f = f0; f < f1; ++f) {
+  int r = g * lines + l;
+  bool row_ok = r < ph;
+  if (row_ok) prefetch_row(r, f);
+  for (long long u = u0; u < u1; ++u) {
     const long long x0 = pos[2 * f], y0 = pos[2 * f + 1];
     const bool ok = window_ok(x0, y0, ph, N, H, W);
     if (row_ok && ok) {
@@ -501,12 +507,21 @@ __global__ void __launch_bounds__(128, 3) base_rows_adjoint_reg(
     }
     __syncwarp();
     reg_fft<N, true, false>(v, buf, t, tw);
-    const bool more = row_ok && f + 1 < f1;
-    if (more) prefetch_row(f + 1);
+    // the next unit
+    const bool more = u + 1 < u1;
+    int gn = g, fn = f + 1;
+    if (fn == nframes) {
+      gn = g + 1;
+      fn = 0;
+    }
+    const int rn = gn * lines + l;
+    const bool pf = more && rn < ph;
+    if (pf) prefetch_row(rn, fn);
     if (row_ok && ok) {
+      const float2* prow = probe + (size_t)r * N;
       float2* grow = grad_sample + (y0 + r) * W + x0;
-      // the object row of this frame; the next scratch row may stay in flight
-      if (more) {
+      // the object row of this unit; the next scratch row may stay in flight
+      if (pf) {
         asm volatile("cp.async.wait_group 1;\n" ::: "memory");
       } else {
         cp_async_wait_all();
@@ -519,10 +534,20 @@ __global__ void __launch_bounds__(128, 3) base_rows_adjoint_reg(
         acc[m] = cadd(acc[m], cmulc(G, obuf[c]));
       }
     }
-  }
-  if (row_ok) {
+    if (!more || gn != g) {
+      // leaving this row group: fold its probe-gradient partial sums into grad_probe
+      if (row_ok) {
 #pragma unroll
-    for (int m = 0; m < S::N1; ++m) atomicAdd(&grad_probe[(size_t)r * N + t + S::T * m], acc[m]);
+        for (int m = 0; m < S::N1; ++m) {
+          atomicAdd(&grad_probe[(size_t)r * N + t + S::T * m], acc[m]);
+          acc[m] = make_float2(0.f, 0.f);
+        }
+      }
+    }
+    g = gn;
+    f = fn;
+    r = rn;
+    row_ok = rn < ph;
   }
 }
 
@@ -651,10 +676,12 @@ void launch_rows_adjoint(const BaseGeom& g, const float2* sample, const float2* 
       using L = RegLaunch<N>;
       const int lines = L::lines(128, g.ph);
       const int rowgroups = (g.ph + lines - 1) / lines;
-      const int fpc = frames_per_cta_for(rowgroups, nframes, sm_count() * 6);
-      dim3 grid(rowgroups, (nframes + fpc - 1) / fpc);
-      base_rows_adjoint_reg<N><<<grid, lines * L::T, L::adj_smem(lines), s>>>(
-          g.scratch, sample, g.H, g.W, probe, g.ph, pos, nframes, fpc, grad_sample, grad_probe, g.row.tw, lines);
+      const int threads = lines * L::T, smem = L::adj_smem(lines);
+      const long long units = (long long)rowgroups * nframes;
+      const int grid = static_cast<int>(
+          std::min<long long>(units, resident_ctas((const void*)base_rows_adjoint_reg<N>, threads, smem)));
+      base_rows_adjoint_reg<N><<<grid, threads, smem, s>>>(g.scratch, sample, g.H, g.W, probe, g.ph, pos, nframes,
+                                                           rowgroups, grad_sample, grad_probe, g.row.tw, lines);
     } else {
       const int rowgroups = (g.ph + g.rs.lines - 1) / g.rs.lines;
       const int fpc = frames_per_cta_for(rowgroups, nframes, sm_count() * 8);

@@ -267,24 +267,30 @@ __global__ void __launch_bounds__(256, 2) coded_rows_pool(
 template <int N>
 __global__ void __launch_bounds__(128, 3) coded_rows_grad_mask(
     float2* __restrict__ scratch, const float2* __restrict__ mask, const float2* __restrict__ xstore, int nframes,
-    int frames_per_cta, float2* __restrict__ grad_mask, const float2* __restrict__ tw, int lines) {
+    int rowgroups, float2* __restrict__ grad_mask, const float2* __restrict__ tw, int lines) {
   using S = RegShape<N>;
   extern __shared__ float2 sm[];
   const int tid = threadIdx.x;
   const int l = tid / S::T;
   const int t = tid - l * S::T;
-  const int r = blockIdx.x * lines + l;
-  const bool row_ok = r < N;
-  const int rr = row_ok ? r : 0;
-  const int f0 = blockIdx.y * frames_per_cta;
-  const int f1 = min(nframes, f0 + frames_per_cta);
+  // (row group, frame) units in row-group-major order; the grid is one wave of resident
+  // CTAs and CTA b takes the contiguous units [u0, u1)
+  const long long units = (long long)rowgroups * nframes;
+  const long long u0 = units * blockIdx.x / gridDim.x;
+  const long long u1 = units * (blockIdx.x + 1) / gridDim.x;
+  if (u0 >= u1) return;
+  int g = static_cast<int>(u0 / nframes);
+  int f = static_cast<int>(u0 - (long long)g * nframes);
   float2* buf = sm + l * RowPass<N>::LP;
   float2* xbuf = sm + lines * RowPass<N>::LP + l * N;
-  const float2* mrow = mask + (size_t)rr * N;
   float2 acc[S::N1];
 #pragma unroll
   for (int m = 0; m < S::N1; ++m) acc[m] = make_float2(0.f, 0.f);
-  for (int f = f0; f < f1; ++f) {
+  for (long long u = u0; u < u1; ++u) {
+    const int r = g * lines + l;
+    const bool row_ok = r < N;
+    const int rr = row_ok ? r : 0;
+    const float2* mrow = mask + (size_t)rr * N;
     const float2* xrow = xstore + ((size_t)f * N + rr) * N;
 #pragma unroll
     for (int m = 0; m < S::N1; ++m) cp_async8(xbuf + t + S::T * m, xrow + t + S::T * m);
@@ -301,10 +307,23 @@ __global__ void __launch_bounds__(128, 3) coded_rows_grad_mask(
     }
     reg_fft<N, false, false>(v, buf, t, tw);
     if (row_ok) store_frame_row<N>(scratch, f, r, v, t);
-  }
-  if (row_ok) {
+    int gn = g, fn = f + 1;
+    if (fn == nframes) {
+      gn = g + 1;
+      fn = 0;
+    }
+    if (u + 1 == u1 || gn != g) {
+      // leaving this row group: fold its mask-gradient partial sums into grad_mask
+      if (row_ok) {
 #pragma unroll
-    for (int m = 0; m < S::N1; ++m) atomicAdd(&grad_mask[(size_t)r * N + t + S::T * m], acc[m]);
+        for (int m = 0; m < S::N1; ++m) {
+          atomicAdd(&grad_mask[(size_t)r * N + t + S::T * m], acc[m]);
+          acc[m] = make_float2(0.f, 0.f);
+        }
+      }
+    }
+    g = gn;
+    f = fn;
   }
 }
 
@@ -455,11 +474,11 @@ void launch_rows_grad_mask(const CodedGeom& g, int nf, const float2* mask, const
     constexpr int N = decltype(NT)::value;
     const int lines = RowPass<N>::lines(128, N);
     const int rowgroups = (N + lines - 1) / lines;
-    const long long ctas_one = (long long)rowgroups * nf;
-    const int fpc = std::max(1, std::min<int>(nf, static_cast<int>(ctas_one / (sm_count() * 6))));
-    dim3 grid(rowgroups, (nf + fpc - 1) / fpc);
-    coded_rows_grad_mask<N><<<grid, lines * RowPass<N>::T, RowPass<N>::smem_with_row(lines), s>>>(
-        g.frames, mask, xstore, nf, fpc, grad_mask, g.plan.tw, lines);
+    const int threads = lines * RowPass<N>::T, smem = RowPass<N>::smem_with_row(lines);
+    const int grid = static_cast<int>(std::min<long long>(
+        (long long)rowgroups * nf, resident_ctas((const void*)coded_rows_grad_mask<N>, threads, smem)));
+    coded_rows_grad_mask<N><<<grid, threads, smem, s>>>(g.frames, mask, xstore, nf, rowgroups, grad_mask, g.plan.tw,
+                                                        lines);
   });
   prof_end(kCodedRows, s);
 }

@@ -10,10 +10,12 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <algorithm>
 #include <atomic>
 #include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <utility>
 #include <vector>
 
@@ -223,6 +225,36 @@ int sm_count() {
     cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
   }
   return n > 0 ? n : 148;
+}
+
+struct ResidentKey {
+  int dev, threads, smem;
+  const void* kernel;
+  bool operator<(const ResidentKey& o) const {
+    return std::tie(dev, threads, smem, kernel) < std::tie(o.dev, o.threads, o.smem, o.kernel);
+  }
+};
+std::mutex g_resident_mutex;
+std::map<ResidentKey, int> g_resident;
+
+int resident_ctas(const void* kernel, int threads, int smem) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const ResidentKey key{dev, threads, smem, kernel};
+  {
+    std::lock_guard<std::mutex> lock(g_resident_mutex);
+    auto it = g_resident.find(key);
+    if (it != g_resident.end()) return it->second;
+  }
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  const int n = std::max(1, per_sm) * sm_count();
+  std::lock_guard<std::mutex> lock(g_resident_mutex);
+  g_resident[key] = n;
+  return n;
 }
 
 }  // namespace ptx

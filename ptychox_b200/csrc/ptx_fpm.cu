@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(256, 2) fpm_cols(
 template <int NW>
 __global__ void __launch_bounds__(128, 3) fpm_rows_adjoint(
     const float2* __restrict__ scratch, const float2* __restrict__ spec, int oh, int ow,
-    const float2* __restrict__ pupil, int lh, const int64_t* __restrict__ led, int nframes, int frames_per_cta,
+    const float2* __restrict__ pupil, int lh, const int64_t* __restrict__ led, int nframes, int rowgroups,
     float norm, float2* __restrict__ grad_spec, float2* __restrict__ grad_pupil, const float2* __restrict__ tw,
     int lines) {
   using S = RegShape<NW>;
@@ -170,18 +170,23 @@ __global__ void __launch_bounds__(128, 3) fpm_rows_adjoint(
   const int tid = threadIdx.x;
   const int l = tid / S::T;
   const int t = tid - l * S::T;
-  const int i = blockIdx.x * lines + l;
-  const bool row_ok = i < lh;
-  const int r = (i + lh / 2) & (lh - 1);
-  const int f0 = blockIdx.y * frames_per_cta;
-  const int f1 = min(nframes, f0 + frames_per_cta);
+  // (row group, frame) units in row-group-major order; the grid is one wave of resident
+  // CTAs and CTA b takes the contiguous units [u0, u1)
+  const long long units = (long long)rowgroups * nframes;
+  const long long u0 = units * blockIdx.x / gridDim.x;
+  const long long u1 = units * (blockIdx.x + 1) / gridDim.x;
+  if (u0 >= u1) return;
+  int g = static_cast<int>(u0 / nframes);
+  int f = static_cast<int>(u0 - (long long)g * nframes);
   float2* buf = sm + l * RowPass<NW>::LP;
   float2* sbuf = sm + lines * RowPass<NW>::LP + l * NW;  // prefetched window row of S
-  const float2* prow = pupil + (size_t)r * NW;
   float2 acc[S::N1];
 #pragma unroll
   for (int m = 0; m < S::N1; ++m) acc[m] = make_float2(0.f, 0.f);
-  for (int f = f0; f < f1; ++f) {
+  for (long long u = u0; u < u1; ++u) {
+    const int i = g * lines + l;
+    const bool row_ok = i < lh;
+    const int r = (i + lh / 2) & (lh - 1);
     const long long lx = led[2 * f], ly = led[2 * f + 1];
     const size_t srow = (size_t)wrap2(ly + r + oh / 2, oh) * ow;
     if (row_ok) {
@@ -207,6 +212,7 @@ __global__ void __launch_bounds__(128, 3) fpm_rows_adjoint(
     }
     reg_fft<NW, false, false>(v, buf, t, tw);
     if (row_ok) {
+      const float2* prow = pupil + (size_t)r * NW;
       cp_async_wait_all();
 #pragma unroll
       for (int m = 0; m < S::N1; ++m) {
@@ -217,13 +223,24 @@ __global__ void __launch_bounds__(128, 3) fpm_rows_adjoint(
         acc[m] = cadd(acc[m], cmulc(gl, sbuf[jj]));
       }
     }
-  }
-  if (row_ok) {
-#pragma unroll
-    for (int m = 0; m < S::N1; ++m) {
-      const int c = (t + S::T * m + NW / 2) & (NW - 1);
-      atomicAdd(&grad_pupil[(size_t)r * NW + c], acc[m]);
+    int gn = g, fn = f + 1;
+    if (fn == nframes) {
+      gn = g + 1;
+      fn = 0;
     }
+    if (u + 1 == u1 || gn != g) {
+      // leaving this row group: fold its pupil-gradient partial sums into grad_pupil
+      if (row_ok) {
+#pragma unroll
+        for (int m = 0; m < S::N1; ++m) {
+          const int c = (t + S::T * m + NW / 2) & (NW - 1);
+          atomicAdd(&grad_pupil[(size_t)r * NW + c], acc[m]);
+          acc[m] = make_float2(0.f, 0.f);
+        }
+      }
+    }
+    g = gn;
+    f = fn;
   }
 }
 
@@ -364,11 +381,11 @@ void launch_rows_adjoint(const FpmGeom& g, const float2* spec, const float2* pup
     constexpr int N = decltype(NT)::value;
     const int lines = RowPass<N>::lines(128, g.lh);
     const int rowgroups = (g.lh + lines - 1) / lines;
-    const long long ctas_one = (long long)rowgroups * nf;
-    const int fpc = std::max(1, std::min<int>(nf, static_cast<int>(ctas_one / (sm_count() * 6))));
-    dim3 grid(rowgroups, (nf + fpc - 1) / fpc);
-    fpm_rows_adjoint<N><<<grid, lines * RowPass<N>::T, RowPass<N>::smem_with_row(lines), s>>>(
-        g.frames, spec, g.oh, g.ow, pupil, g.lh, led, nf, fpc, norm, grad_spec, grad_pupil, g.p_lw.tw, lines);
+    const int threads = lines * RowPass<N>::T, smem = RowPass<N>::smem_with_row(lines);
+    const int grid = static_cast<int>(std::min<long long>(
+        (long long)rowgroups * nf, resident_ctas((const void*)fpm_rows_adjoint<N>, threads, smem)));
+    fpm_rows_adjoint<N><<<grid, threads, smem, s>>>(g.frames, spec, g.oh, g.ow, pupil, g.lh, led, nf, rowgroups,
+                                                    norm, grad_spec, grad_pupil, g.p_lw.tw, lines);
   });
   prof_end(kFpmRowsAdjoint, s);
 }

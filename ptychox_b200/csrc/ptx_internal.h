@@ -45,6 +45,11 @@ ColShape col_shape(const LinePlan& p);
 
 int sm_count();
 
+// CTAs of `kernel` (launched with `threads` threads and `smem` dynamic shared bytes) that
+// the current device holds at once: SMs x resident CTAs per SM, at least 1.  Cached per
+// (device, kernel, threads, smem).
+int resident_ctas(const void* kernel, int threads, int smem);
+
 // Kernel kinds for the launch counter and the optional per-kernel event profiler.
 enum KernelId {
   kBaseRowsForward = 0,
