@@ -9,7 +9,8 @@
  *     stream-ordered and nothing synchronises the host;
  *   - outputs are caller-allocated; temporary frames live in a caller-provided
  *     workspace whose minimum size the *_workspace_bytes functions return (a larger
- *     workspace processes more frames per launch);
+ *     workspace processes more frames per launch); the workspace must start on a
+ *     256-byte boundary (cudaMalloc and PyTorch allocations do);
  *   - the return value is a status code (PTX_OK = 0); ptx_last_error() gives the
  *     calling thread's last message.
  *

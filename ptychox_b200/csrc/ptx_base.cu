@@ -260,44 +260,101 @@ struct RowCfg {
 };
 
 // Row pass 1 (register FFT): gather O rows x probe rows, forward row DFT, store tiled.
+// Work units are (row group, frame) pairs in row-group-major order over one wave of
+// resident CTAs (CTA b takes the contiguous units [u0, u1)).  The probe rows of the
+// current row group and the twiddle table sit in shared memory; each unit's object rows
+// arrive by 16-byte cp.async that bypasses L1 (evict-last in L2, the object is re-read by
+// every frame) into the line buffer, and the next unit's rows are requested as soon as
+// this unit's transform has released the buffer, so they land while it stores.
 template <int N>
-__global__ void __launch_bounds__(256, 2) base_rows_forward_reg(
+struct FwdCfg {
+  static constexpr int BP = RowCfg<N>::LP > N + 2 ? RowCfg<N>::LP : N + 2;
+  static_assert(BP % 2 == 0, "16-byte landing lines");
+  static int smem(int lines) { return (lines * (BP + N) + N) * (int)sizeof(float2); }
+};
+
+template <int N>
+__global__ void __launch_bounds__(128, 3) base_rows_forward_reg(
     const float2* __restrict__ sample, int H, int W, const float2* __restrict__ probe, int ph,
-    const int64_t* __restrict__ pos, float2* __restrict__ scratch, const float2* __restrict__ tw, int lines,
-    unsigned* __restrict__ err) {
+    const int64_t* __restrict__ pos, int nframes, int rowgroups, float2* __restrict__ scratch,
+    const float2* __restrict__ tw, int lines, unsigned* __restrict__ err) {
   using S = RegShape<N>;
+  using Cfg = FwdCfg<N>;
   constexpr int kTiles = N / kTile;
   extern __shared__ float2 sm[];
   const int tid = threadIdx.x;
   const int l = tid / S::T;
   const int t = tid - l * S::T;
-  const int r = blockIdx.x * lines + l;
-  const int f = blockIdx.y;
-  const bool row_ok = r < ph;
-  const long long x0 = pos[2 * f], y0 = pos[2 * f + 1];
-  const bool ok = window_ok(x0, y0, ph, N, H, W);
-  if (!ok && tid == 0 && blockIdx.x == 0) atomicOr(err, 1u);
-  float2 v[S::N1];
-  if (ok && row_ok) {
-    const float2* orow = sample + (y0 + r) * W + x0;
-    const float2* prow = probe + (size_t)r * N;
+  const long long units = (long long)rowgroups * nframes;
+  const long long u0 = units * blockIdx.x / gridDim.x;
+  const long long u1 = units * (blockIdx.x + 1) / gridDim.x;
+  if (u0 >= u1) return;
+  int g = static_cast<int>(u0 / nframes);
+  int f = static_cast<int>(u0 - (long long)g * nframes);
+  float2* buf = sm + l * Cfg::BP;
+  float2* pbuf = sm + lines * Cfg::BP + l * N;
+  float2* tws = sm + lines * (Cfg::BP + N);
+  for (int i = tid; i < N; i += blockDim.x) tws[i] = __ldg(&tw[i]);
+  __syncthreads();
+  const uint64_t pol_last = policy_evict_last();
+  // object row of unit (row, frame) into buf; returns its shift (or -1 when not copied)
+  auto request = [&](int row, int frame) -> int {
+    const long long x0 = pos[2 * frame], y0 = pos[2 * frame + 1];
+    if (row >= ph || !window_ok(x0, y0, ph, N, H, W)) return -1;
+    const float2* orow = sample + (y0 + row) * W + x0;
+    const int s = half_shift(orow);
+    copy_row_shifted<N>(buf, orow, s, t, pol_last);
+    cp_async_commit();
+    return s;
+  };
+  int r = g * lines + l;
+  int shift = request(r, f);
+  bool new_group = true;
+  for (long long u = u0; u < u1; ++u) {
+    const bool row_ok = r < ph;
+    if (tid == 0 && !window_ok(pos[2 * f], pos[2 * f + 1], ph, N, H, W)) atomicOr(err, 1u);
+    if (new_group && row_ok) {
+      // probe row of the new row group (each thread copies and later reads its own elements)
 #pragma unroll
-    for (int j = 0; j < S::N1; ++j) {
-      const int c = t + S::T * j;
-      v[j] = cmul(orow[c], __ldg(&prow[c]));
+      for (int m = 0; m < S::N1; ++m) pbuf[t + S::T * m] = __ldg(&probe[(size_t)r * N + t + S::T * m]);
     }
-  } else {
+    new_group = false;
+    cp_async_wait_all();
+    __syncwarp();
+    float2 v[S::N1];
+    if (shift >= 0) {
 #pragma unroll
-    for (int j = 0; j < S::N1; ++j) v[j] = make_float2(0.f, 0.f);
-  }
-  reg_fft<N, false, false>(v, sm + l * RowCfg<N>::LP, t, tw);
-  if (row_ok) {
-    float2* base = scratch + (size_t)f * kTiles * ph * kTile + (size_t)r * kTile;
+      for (int j = 0; j < S::N1; ++j) {
+        const int c = t + S::T * j;
+        v[j] = cmul(buf[c + shift], pbuf[c]);
+      }
+    } else {
 #pragma unroll
-    for (int m = 0; m < S::N1; ++m) {
-      const int kc = t + S::T * m;
-      base[(size_t)(kc / kTile) * ph * kTile + (kc % kTile)] = v[m];
+      for (int j = 0; j < S::N1; ++j) v[j] = make_float2(0.f, 0.f);
     }
+    __syncwarp();
+    reg_fft<N, false, false, true>(v, buf, t, tws);
+    const bool more = u + 1 < u1;
+    int gn = g, fn = f + 1;
+    if (fn == nframes) {
+      gn = g + 1;
+      fn = 0;
+    }
+    const int rn = gn * lines + l;
+    const int shift_next = more ? request(rn, fn) : -1;
+    if (row_ok) {
+      float2* base = scratch + (size_t)f * kTiles * ph * kTile + (size_t)r * kTile;
+#pragma unroll
+      for (int m = 0; m < S::N1; ++m) {
+        const int kc = t + S::T * m;
+        base[(size_t)(kc / kTile) * ph * kTile + (kc % kTile)] = v[m];
+      }
+    }
+    if (gn != g) new_group = true;
+    g = gn;
+    f = fn;
+    r = rn;
+    shift = shift_next;
   }
 }
 
@@ -436,69 +493,95 @@ __global__ void __launch_bounds__(256, 2) base_cols_reg(
   }
 }
 
-// Row pass 2 (register FFT): inverse row DFT, scatter G conj(P) into grad_O, accumulate
-// G conj(O) for grad_P in registers across this CTA's frames.
+// Shared memory of the adjoint row pass, per line: the exchange / scratch landing line
+// (BP), the object row (OP = N + 2: a 16-byte aligned copy shifted by the row's 8-byte
+// misalignment) and the probe row (N); per CTA: the twiddle table (N).
 template <int N>
-__global__ void __launch_bounds__(128, 3) base_rows_adjoint_reg(
+struct AdjCfg {
+  static constexpr int BP = RowCfg<N>::LP > N ? RowCfg<N>::LP : N;
+  static constexpr int OP = N + 2;
+  static_assert(BP % 2 == 0, "16-byte landing lines");
+  static int smem(int lines) { return (lines * (BP + OP + N) + N) * (int)sizeof(float2); }
+};
+
+// Row pass 2 (register FFT): inverse row DFT, scatter G conj(P) into grad_O, accumulate
+// G conj(O) for grad_P in registers.  Work units are (row group, frame) pairs in
+// row-group-major order; the grid is one wave of resident CTAs and CTA b takes the
+// contiguous units [u0, u1), so every CTA does the same number of frame-rows and covers at
+// most a few row groups.  Per unit the scratch rows and the object rows arrive by 16-byte
+// cp.async that bypasses L1 (scratch marked evict-first in L2, the object evict-last), so
+// L1 is left to the atomics; the probe rows of the current row group and the twiddle
+// table sit in shared memory.  The next unit's scratch row lands while this unit scatters.
+template <int N>
+__global__ void __launch_bounds__(128, 2) base_rows_adjoint_reg(
     const float2* __restrict__ scratch, const float2* __restrict__ sample, int H, int W,
     const float2* __restrict__ probe, int ph, const int64_t* __restrict__ pos, int nframes, int rowgroups,
     float2* __restrict__ grad_sample, float2* __restrict__ grad_probe, const float2* __restrict__ tw, int lines) {
   using S = RegShape<N>;
+  using Cfg = AdjCfg<N>;
   constexpr int kTiles = N / kTile;
   extern __shared__ float2 sm[];
   const int tid = threadIdx.x;
   const int l = tid / S::T;
   const int t = tid - l * S::T;
-  // Work units are (row group, frame) pairs in row-group-major order; the grid is one wave
-  // of resident CTAs and CTA b takes the contiguous units [u0, u1), so every CTA does the
-  // same number of frame-rows and each covers at most a few row groups.
   const long long units = (long long)rowgroups * nframes;
   const long long u0 = units * blockIdx.x / gridDim.x;
   const long long u1 = units * (blockIdx.x + 1) / gridDim.x;
   if (u0 >= u1) return;
   int g = static_cast<int>(u0 / nframes);
   int f = static_cast<int>(u0 - (long long)g * nframes);
-  // line buffer: the FFT's exchange buffer, and between transforms the landing place of
-  // the next unit's scratch row (prefetched with cp.async while this unit scatters)
-  constexpr int BP = RowCfg<N>::LP > N ? RowCfg<N>::LP : N;
-  float2* buf = sm + l * BP;
-  // this line's object row, prefetched with cp.async (each thread copies and later reads
-  // exactly the elements it owns, so only its own copies need waiting for)
-  float2* obuf = sm + lines * BP + l * N;
+  float2* buf = sm + l * Cfg::BP;
+  float2* obuf = sm + lines * Cfg::BP + l * Cfg::OP;
+  float2* pbuf = sm + lines * (Cfg::BP + Cfg::OP) + l * N;
+  float2* tws = sm + lines * (Cfg::BP + Cfg::OP + N);
+  for (int i = tid; i < N; i += blockDim.x) tws[i] = __ldg(&tw[i]);
+  __syncthreads();
+  const uint64_t pol_first = policy_evict_first();
+  const uint64_t pol_last = policy_evict_last();
   float2 acc[S::N1];
 #pragma unroll
   for (int m = 0; m < S::N1; ++m) acc[m] = make_float2(0.f, 0.f);
-  // thread t copies / reads the scratch elements c = t + T j of its row (same ownership
-  // as the FFT input), so each thread only waits for its own copies
+  // the scratch row (row, frame) into buf: N/2 16-byte chunks, chunk q = t + T i
   auto prefetch_row = [&](int row, int frame) {
     const float2* base = scratch + (size_t)frame * kTiles * ph * kTile + (size_t)row * kTile;
 #pragma unroll
-    for (int j = 0; j < S::N1; ++j) {
-      const int c = t + S::T * j;
-      cp_async8(buf + c, base + (size_t)(c / kTile) * ph * kTile + (c % kTile));
+    for (int i = 0; i < S::N1 / 2; ++i) {
+      const int c = 2 * (t + S::T * i);
+      cp_async16_hint(buf + c, base + (size_t)(c / kTile) * ph * kTile + (c % kTile), pol_first);
     }
     cp_async_commit();
   };
   int r = g * lines + l;
   bool row_ok = r < ph;
+  bool new_group = true;
   if (row_ok) prefetch_row(r, f);
   for (long long u = u0; u < u1; ++u) {
     const long long x0 = pos[2 * f], y0 = pos[2 * f + 1];
     const bool ok = window_ok(x0, y0, ph, N, H, W);
+    const float2* orow = sample + (y0 + r) * W + x0;
+    const int shift = half_shift(orow);
     if (row_ok && ok) {
-      const float2* orow = sample + (y0 + r) * W + x0;
-#pragma unroll
-      for (int m = 0; m < S::N1; ++m) cp_async8(obuf + t + S::T * m, orow + t + S::T * m);
+      copy_row_shifted<N>(obuf, orow, shift, t, pol_last);
       cp_async_commit();
     }
+    if (new_group && row_ok) {
+      // probe row of the new row group (each thread copies and later reads its own elements)
+#pragma unroll
+      for (int m = 0; m < S::N1; ++m) pbuf[t + S::T * m] = __ldg(&probe[(size_t)r * N + t + S::T * m]);
+    }
+    new_group = false;
     float2 v[S::N1];
     if (row_ok) {
-      // wait for the scratch row (committed before the object row)
+      // the scratch row (committed before the object row); other lanes of the line copied
+      // part of it, so the line's lanes meet at a warp barrier before reading
       if (ok) {
         asm volatile("cp.async.wait_group 1;\n" ::: "memory");
       } else {
         cp_async_wait_all();
       }
+    }
+    __syncwarp();
+    if (row_ok) {
 #pragma unroll
       for (int j = 0; j < S::N1; ++j) v[j] = buf[t + S::T * j];
     } else {
@@ -506,8 +589,7 @@ __global__ void __launch_bounds__(128, 3) base_rows_adjoint_reg(
       for (int j = 0; j < S::N1; ++j) v[j] = make_float2(0.f, 0.f);
     }
     __syncwarp();
-    reg_fft<N, true, false>(v, buf, t, tw);
-    // the next unit
+    reg_fft<N, true, false, true>(v, buf, t, tws);
     const bool more = u + 1 < u1;
     int gn = g, fn = f + 1;
     if (fn == nframes) {
@@ -518,24 +600,24 @@ __global__ void __launch_bounds__(128, 3) base_rows_adjoint_reg(
     const bool pf = more && rn < ph;
     if (pf) prefetch_row(rn, fn);
     if (row_ok && ok) {
-      const float2* prow = probe + (size_t)r * N;
       float2* grow = grad_sample + (y0 + r) * W + x0;
-      // the object row of this unit; the next scratch row may stay in flight
       if (pf) {
         asm volatile("cp.async.wait_group 1;\n" ::: "memory");
       } else {
         cp_async_wait_all();
       }
+      __syncwarp();
 #pragma unroll
       for (int m = 0; m < S::N1; ++m) {
         const int c = t + S::T * m;
         const float2 G = v[m];
-        atomicAdd(&grow[c], cmulc(G, __ldg(&prow[c])));
-        acc[m] = cadd(acc[m], cmulc(G, obuf[c]));
+        atomicAdd(&grow[c], cmulc(G, pbuf[c]));
+        acc[m] = cadd(acc[m], cmulc(G, obuf[c + shift]));
       }
+    } else {
+      __syncwarp();
     }
     if (!more || gn != g) {
-      // leaving this row group: fold its probe-gradient partial sums into grad_probe
       if (row_ok) {
 #pragma unroll
         for (int m = 0; m < S::N1; ++m) {
@@ -543,6 +625,7 @@ __global__ void __launch_bounds__(128, 3) base_rows_adjoint_reg(
           acc[m] = make_float2(0.f, 0.f);
         }
       }
+      new_group = true;
     }
     g = gn;
     f = fn;
@@ -562,9 +645,7 @@ struct RegLaunch {
     return l < need ? l : need;
   }
   static int row_smem(int lines) { return lines * RowCfg<N>::LP * (int)sizeof(float2); }
-  static int adj_smem(int lines) {
-    return lines * ((RowCfg<N>::LP > N ? RowCfg<N>::LP : N) + N) * (int)sizeof(float2);
-  }
+  static int adj_smem(int lines) { return AdjCfg<N>::smem(lines); }
   static int col_threads() { return kColsReg * T; }
   static int col_smem() { return ColCfg<N>::kSmemBytes; }
 };
@@ -588,6 +669,9 @@ int check_common(const void* sample, int H, int W, const void* probe, int ph, in
   }
   if (H <= 0 || W <= 0 || ph <= 0 || pw <= 0 || batch < 0) {
     return set_error(PTX_ERR_INVALID_ARGUMENT, "non-positive shape");
+  }
+  if (reinterpret_cast<uintptr_t>(ws) & 255) {
+    return set_error(PTX_ERR_INVALID_ARGUMENT, "workspace must start on a 256-byte boundary");
   }
   if (ph > H || pw > W) {
     return set_error(PTX_ERR_INVALID_ARGUMENT, "probe (%d x %d) larger than sample (%d x %d)", ph, pw, H, W);
@@ -616,7 +700,7 @@ int check_common(const void* sample, int H, int W, const void* probe, int ph, in
     constexpr int N = decltype(NT)::value;
     if constexpr (N > 0) {
       using L = RegLaunch<N>;
-      if (!st) st = ensure_smem((const void*)base_rows_forward_reg<N>, L::row_smem(L::lines(256, ph)));
+      if (!st) st = ensure_smem((const void*)base_rows_forward_reg<N>, FwdCfg<N>::smem(L::lines(128, ph)));
       if (!st) st = ensure_smem((const void*)base_rows_adjoint_reg<N>, L::adj_smem(L::lines(128, ph)));
     } else {
       if (!st) st = ensure_smem((const void*)base_rows_forward_rt<0>, g->rs.smem);
@@ -653,10 +737,13 @@ void launch_rows_forward(const BaseGeom& g, const float2* sample, const float2* 
     constexpr int N = decltype(NT)::value;
     if constexpr (N > 0) {
       using L = RegLaunch<N>;
-      const int lines = L::lines(256, g.ph);
-      dim3 grid((g.ph + lines - 1) / lines, nframes);
-      base_rows_forward_reg<N><<<grid, lines * L::T, L::row_smem(lines), s>>>(sample, g.H, g.W, probe, g.ph, pos,
-                                                                             g.scratch, g.row.tw, lines, g.err);
+      const int lines = L::lines(128, g.ph);
+      const int rowgroups = (g.ph + lines - 1) / lines;
+      const int threads = lines * L::T, smem = FwdCfg<N>::smem(lines);
+      const int grid = static_cast<int>(std::min<long long>(
+          (long long)rowgroups * nframes, resident_ctas((const void*)base_rows_forward_reg<N>, threads, smem)));
+      base_rows_forward_reg<N><<<grid, threads, smem, s>>>(sample, g.H, g.W, probe, g.ph, pos, nframes, rowgroups,
+                                                           g.scratch, g.row.tw, lines, g.err);
     } else {
       const int rowgroups = (g.ph + g.rs.lines - 1) / g.rs.lines;
       dim3 grid(rowgroups, nframes);

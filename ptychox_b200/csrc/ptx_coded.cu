@@ -358,6 +358,9 @@ int coded_check(int n, int ds, const void* a, const void* b, const void* t2, con
                 size_t ws_bytes, bool need_xstore, CodedGeom* g) {
   if (!a || !b || !t2 || (!shifts && batch > 0) || !ws) return set_error(PTX_ERR_INVALID_ARGUMENT, "null pointer argument");
   if (batch < 0) return set_error(PTX_ERR_INVALID_ARGUMENT, "negative batch");
+  if (reinterpret_cast<uintptr_t>(ws) & 255) {
+    return set_error(PTX_ERR_INVALID_ARGUMENT, "workspace must start on a 256-byte boundary");
+  }
   if (!is_pow2_len(n) || n < 16) {
     return set_error(PTX_ERR_UNSUPPORTED_SIZE, "coded field side must be a power of two in [16, 1024] (got %d)", n);
   }

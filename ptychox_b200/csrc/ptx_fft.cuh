@@ -64,6 +64,30 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
+// L2 eviction policies for the cache-hinted copies below: streamed data (scratch frames)
+// evict-first, data re-read across frames (object, spectrum) evict-last.
+__device__ __forceinline__ uint64_t policy_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t policy_evict_last() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;\n" : "=l"(p));
+  return p;
+}
+// 16-byte global -> shared copy that bypasses L1, with an L2 eviction policy
+__device__ __forceinline__ void cp_async16_hint(void* smem, const void* gmem, uint64_t pol) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async8_hint(void* smem, const void* gmem, uint64_t pol) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "l"(pol)
+               : "memory");
+}
+
 // multiply by -i (forward transform) or +i (inverse transform)
 template <bool INV>
 __device__ __forceinline__ float2 mul_i(float2 z) {

@@ -270,6 +270,9 @@ int fpm_check(const void* object, int oh, int ow, const void* pupil, int lh, int
               void* ws, size_t ws_bytes, FpmGeom* g) {
   if (!object || !pupil || (!led && batch > 0) || !ws) return set_error(PTX_ERR_INVALID_ARGUMENT, "null pointer argument");
   if (batch < 0) return set_error(PTX_ERR_INVALID_ARGUMENT, "negative batch");
+  if (reinterpret_cast<uintptr_t>(ws) & 255) {
+    return set_error(PTX_ERR_INVALID_ARGUMENT, "workspace must start on a 256-byte boundary");
+  }
   for (int n : {oh, ow, lh, lw}) {
     if (!is_pow2_len(n)) {
       return set_error(PTX_ERR_UNSUPPORTED_SIZE, "FPM sides must be powers of two in [4, 1024] (got %d)", n);

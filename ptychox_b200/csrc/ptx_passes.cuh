@@ -13,6 +13,36 @@ namespace ptx {
 constexpr float kEpsF32 = 1.1920928955078125e-07f;  // torch.finfo(float32).eps
 constexpr int kColsPerCta = 8;                        // columns per column-pass CTA
 
+// Copy the N-element row `src` (float2, 8-byte aligned) into `dst` with 16-byte cp.async
+// that bypasses L1, element c landing at dst[c + s], s = 1 when src sits 8 bytes past a
+// 16-byte boundary (dst must be 16-byte aligned and hold N + 2 elements).  A shifted row
+// copies its first and last elements singly so no access leaves the row.  Thread t of the
+// T threads of a line copies chunks t + T i; the caller commits, waits and then meets the
+// other lanes at a barrier before reading.
+template <int N>
+__device__ __forceinline__ void copy_row_shifted(float2* dst, const float2* src, int s, int t, uint64_t pol) {
+  using S = RegShape<N>;
+  if (s == 0) {
+#pragma unroll
+    for (int i = 0; i < S::N1 / 2; ++i) {
+      const int c = 2 * (t + S::T * i);
+      cp_async16_hint(dst + c, src + c, pol);
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < S::N1 / 2; ++i) {
+      const int c = 1 + 2 * (t + S::T * i);
+      if (c + 1 < N) cp_async16_hint(dst + c + 1, src + c, pol);
+    }
+    if (t == 0) cp_async8_hint(dst + 1, src, pol);
+    if (t == S::T - 1) cp_async8_hint(dst + N, src + N - 1, pol);
+  }
+}
+// 8-byte offset of p from a 16-byte boundary, in float2 elements (0 or 1)
+__device__ __forceinline__ int half_shift(const float2* p) {
+  return static_cast<int>((reinterpret_cast<uintptr_t>(p) >> 3) & 1);
+}
+
 template <int N>
 struct RowPass {
   static constexpr int T = RegShape<N>::T;

@@ -187,15 +187,16 @@ __device__ __forceinline__ void line_sync() {
 // Transform the line owned by threads t = 0..T-1 in place (see the file comment for the
 // layout).  `buf` is this line's exchange buffer (RegShape<N>::BUF float2).  BLOCK
 // selects a block-wide barrier (lines spread over several warps) instead of a warp one;
-// every thread of the block (or warp) must call it.
-template <int N, bool INV, bool BLOCK>
+// every thread of the block (or warp) must call it.  TW_SHARED: `tw` points to a copy of
+// the twiddle table in shared memory (read with plain loads) instead of global memory.
+template <int N, bool INV, bool BLOCK, bool TW_SHARED = false>
 __device__ __forceinline__ void reg_fft(float2 (&v)[RegShape<N>::N1], float2* buf, int t,
                                         const float2* __restrict__ tw) {
   using S = RegShape<N>;
   RegDft<S::N1, INV>::run(v);
 #pragma unroll
   for (int k1 = 1; k1 < S::N1; ++k1) {
-    float2 w = __ldg(&tw[t * k1]);
+    float2 w = TW_SHARED ? tw[t * k1] : __ldg(&tw[t * k1]);
     if (INV) w.y = -w.y;
     v[k1] = cmul(v[k1], w);
   }
