@@ -88,6 +88,16 @@ __device__ __forceinline__ void cp_async8_hint(void* smem, const void* gmem, uin
                : "memory");
 }
 
+// 16-byte global load that does not allocate in L1, with an L2 eviction policy (streamed
+// scratch elements that this thread reads once)
+__device__ __forceinline__ float4 ld_stream4(const float2* p, uint64_t pol) {
+  float4 v;
+  asm("ld.global.L1::no_allocate.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;\n"
+      : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+      : "l"(p), "l"(pol));
+  return v;
+}
+
 // multiply by -i (forward transform) or +i (inverse transform)
 template <bool INV>
 __device__ __forceinline__ float2 mul_i(float2 z) {

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "ptx_pairfft.cuh"
 #include "ptx_regfft.cuh"
 
 namespace ptx {

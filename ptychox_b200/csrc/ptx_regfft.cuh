@@ -33,7 +33,7 @@ struct RegShape {
 
 // cos(2 pi m / 32) and sin(2 pi m / 32), m in [0, 32): after unrolling, m is a compile-time
 // constant and the switch folds to an immediate.
-__device__ __forceinline__ float cos32(int m) {
+__host__ __device__ __forceinline__ float cos32(int m) {
   switch (m & 31) {
     case 0: return 1.0f;
     case 1: return 0.9807852804032304f;
@@ -70,7 +70,7 @@ __device__ __forceinline__ float cos32(int m) {
     default: return 0.f;
   }
 }
-__device__ __forceinline__ float sin32(int m) {
+__host__ __device__ __forceinline__ float sin32(int m) {
   switch (m & 31) {
     case 0: return 0.0f;
     case 1: return 0.19509032201612825f;
