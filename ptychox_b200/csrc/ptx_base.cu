@@ -294,7 +294,7 @@ __global__ void __launch_bounds__(128, 3) base_rows_forward_reg(
   float2* buf = sm + l * Cfg::BP;
   float2* pbuf = sm + lines * Cfg::BP + l * N;
   float2* tws = sm + lines * (Cfg::BP + N);
-  for (int i = tid; i < N; i += blockDim.x) tws[i] = __ldg(&tw[i]);
+  load_twiddles_by_thread<N>(tws, tw);
   __syncthreads();
   const uint64_t pol_last = policy_evict_last();
   // object row of unit (row, frame) into buf; returns its shift (or -1 when not copied)
@@ -640,7 +640,7 @@ __global__ void __launch_bounds__(128, 2) base_rows_adjoint_reg(
   float2* obuf = sm + lines * Cfg::BP + l * Cfg::OP;
   float2* pbuf = sm + lines * (Cfg::BP + Cfg::OP) + l * N;
   float2* tws = sm + lines * (Cfg::BP + Cfg::OP + N);
-  for (int i = tid; i < N; i += blockDim.x) tws[i] = __ldg(&tw[i]);
+  load_twiddles_by_thread<N>(tws, tw);
   __syncthreads();
   const uint64_t pol_first = policy_evict_first();
   const uint64_t pol_last = policy_evict_last();

@@ -175,6 +175,18 @@ __host__ __device__ constexpr int col_line_pitch() {
   return RegShape<N>::BUF + ((2 - RegShape<N>::BUF % 16) + 16) % 16;
 }
 
+// Fill the shared-memory table of reg_fft<..., TW_SHARED = true> from the global table
+// exp(-2 pi i m / N): entry k1 * T + t holds m = t * k1 (always < N).  All threads of the
+// block call it; the caller synchronises before use.
+template <int N>
+__device__ __forceinline__ void load_twiddles_by_thread(float2* dst, const float2* __restrict__ tw) {
+  using S = RegShape<N>;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    const int k1 = i / S::T, t = i - k1 * S::T;
+    dst[i] = __ldg(&tw[t * k1]);
+  }
+}
+
 template <bool BLOCK>
 __device__ __forceinline__ void line_sync() {
   if (BLOCK) {
@@ -187,8 +199,9 @@ __device__ __forceinline__ void line_sync() {
 // Transform the line owned by threads t = 0..T-1 in place (see the file comment for the
 // layout).  `buf` is this line's exchange buffer (RegShape<N>::BUF float2).  BLOCK
 // selects a block-wide barrier (lines spread over several warps) instead of a warp one;
-// every thread of the block (or warp) must call it.  TW_SHARED: `tw` points to a copy of
-// the twiddle table in shared memory (read with plain loads) instead of global memory.
+// every thread of the block (or warp) must call it.  TW_SHARED: `tw` points to a
+// shared-memory table laid out by thread, tw[k1 * T + t] = exp(-2 pi i t k1 / N) (see
+// load_twiddles_by_thread), so the T lanes of a line read consecutive words.
 template <int N, bool INV, bool BLOCK, bool TW_SHARED = false>
 __device__ __forceinline__ void reg_fft(float2 (&v)[RegShape<N>::N1], float2* buf, int t,
                                         const float2* __restrict__ tw) {
@@ -196,7 +209,7 @@ __device__ __forceinline__ void reg_fft(float2 (&v)[RegShape<N>::N1], float2* bu
   RegDft<S::N1, INV>::run(v);
 #pragma unroll
   for (int k1 = 1; k1 < S::N1; ++k1) {
-    float2 w = TW_SHARED ? tw[t * k1] : __ldg(&tw[t * k1]);
+    float2 w = TW_SHARED ? tw[k1 * S::T + t] : __ldg(&tw[t * k1]);
     if (INV) w.y = -w.y;
     v[k1] = cmul(v[k1], w);
   }
