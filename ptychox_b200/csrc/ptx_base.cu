@@ -493,112 +493,6 @@ __global__ void __launch_bounds__(256, 2) base_cols_reg(
   }
 }
 
-// Column pass of the fused sweep on the two-line packed-FP32x2 FFT (ptx_pairfft.cuh).  A
-// CTA owns one 16-column tile of one frame; thread (p, t) transforms the column pair
-// (2p, 2p+1) of the tile, both columns in lock-step, so every butterfly, twiddle product
-// and epilogue operation is one packed instruction for two columns.  A column pair is one
-// 16-byte load / store per row (a warp covers four whole 128-byte tile rows).  The counts
-// of the tile (fftshifted) arrive by cp.async while the forward transform runs; the
-// twiddle table is kept in shared memory as broadcast pairs (w.x, w.x, w.y, w.y).
-template <int N>
-struct ColPairCfg {
-  static constexpr int kPairs = kTile / 2;
-  static constexpr int LP4 = RegShape<N>::BUF + 1;  // odd float4 pitch: quarter-warps conflict-free
-  static constexpr int kThreads = kPairs * RegShape<N>::T;
-  static constexpr int kExchBytes = kPairs * LP4 * (int)sizeof(float4);
-  static constexpr int kTwBytes = N * (int)sizeof(float4);
-  static constexpr int kMeasBytes = N * kTile * (int)sizeof(uint16_t);
-  static constexpr int kSmemBytes = kExchBytes + kTwBytes + kMeasBytes;
-};
-
-template <int N>
-__global__ void __launch_bounds__(ColPairCfg<N>::kThreads, ColPairCfg<N>::kThreads <= 128 ? 2 : 1) base_cols_pair(
-    float2* __restrict__ scratch, int pw, int frame0, const float2* __restrict__ tw,
-    const uint16_t* __restrict__ measured, const float* __restrict__ lut, float grad_scale, double inv_numel,
-    double* __restrict__ loss) {
-  using S = RegShape<N>;
-  using Cfg = ColPairCfg<N>;
-  extern __shared__ float4 sm4[];
-  float4* tw4 = sm4 + Cfg::kPairs * Cfg::LP4;
-  uint16_t* meas_s = reinterpret_cast<uint16_t*>(tw4 + N);
-  const int tid = threadIdx.x;
-  const int p = tid % Cfg::kPairs;
-  const int t = tid / Cfg::kPairs;
-  const int ct = blockIdx.x;
-  const int f = blockIdx.y;
-  const int c0 = ct * kTile;
-  const bool okA = c0 + 2 * p < pw;
-  const bool okB = c0 + 2 * p + 1 < pw;
-  float2* tile = scratch + ((size_t)f * num_tiles(pw) + ct) * N * kTile + 2 * p;
-  const size_t g = (size_t)frame0 + f;
-  float4* buf = sm4 + p * Cfg::LP4;
-
-  // counts of rows kr (unshifted) of the tile -> meas_s[kr][16]
-  int ic0 = c0 + pw / 2;
-  if (ic0 >= pw) ic0 -= pw;
-  const bool fast = (pw % (2 * kTile) == 0) && ((reinterpret_cast<uintptr_t>(measured) & 15) == 0);
-  if (fast) {
-    for (int i = tid; i < 2 * N; i += blockDim.x) {
-      const int kr = i >> 1, h = (i & 1) * 8;
-      const int ir = (kr + N / 2) & (N - 1);
-      cp_async16(meas_s + kr * kTile + h, measured + (g * N + ir) * pw + ic0 + h);
-    }
-    cp_async_commit();
-  } else {
-    for (int i = tid; i < N * kTile; i += blockDim.x) {
-      const int kr = i / kTile, cc = i - kr * kTile;
-      const int ir = (kr + N / 2) & (N - 1);
-      int icc = c0 + cc + pw / 2;
-      if (icc >= pw) icc -= pw;
-      meas_s[i] = (c0 + cc < pw) ? measured[(g * N + ir) * pw + icc] : 0;
-    }
-  }
-  for (int i = tid; i < N; i += blockDim.x) {
-    const float2 w = __ldg(&tw[i]);
-    tw4[i] = make_float4(w.x, w.x, w.y, w.y);
-  }
-  const uint64_t pol = policy_evict_first();
-  CPair v[S::N1];
-#pragma unroll
-  for (int j = 0; j < S::N1; ++j) {
-    float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (okA) q = ld_stream4(tile + (t + S::T * j) * kTile, pol);
-    if (!okB) q.z = q.w = 0.f;
-    v[j] = {make_float2(q.x, q.z), make_float2(q.y, q.w)};
-  }
-  __syncthreads();  // twiddle table
-  pair_fft<N, false, true>(v, buf, t, tw4);
-  cp_async_wait_all();
-  __syncthreads();
-  float2 part = make_float2(0.f, 0.f);  // squared residuals of the two columns
-  const float2 gs = f2(grad_scale);
-#pragma unroll
-  for (int m = 0; m < S::N1; ++m) {
-    const int kr = t + S::T * m;
-    const CPair F = v[m];
-    const float2 s2 = fma2(F.re, F.re, mul2(F.im, F.im));
-    const float2 r = make_float2(rsqrt_nr(fmaxf(s2.x, 1e-37f)), rsqrt_nr(fmaxf(s2.y, 1e-37f)));
-    const float2 a = mul2(s2, r);
-    const float2 inv = make_float2(a.x >= kEps ? r.x : 1.0f / kEps, a.y >= kEps ? r.y : 1.0f / kEps);
-    const uint32_t cnt = *reinterpret_cast<const uint32_t*>(meas_s + kr * kTile + 2 * p);
-    const float2 y = make_float2(okA ? __ldg(&lut[cnt & 0xffffu]) : 0.f, okB ? __ldg(&lut[cnt >> 16]) : 0.f);
-    float2 rr = sub2(a, y);
-    rr = make_float2(okA ? rr.x : 0.f, okB ? rr.y : 0.f);
-    part = fma2(rr, rr, part);
-    const float2 sc = mul2(mul2(gs, rr), inv);
-    v[m] = {mul2(F.re, sc), mul2(F.im, sc)};
-  }
-  pair_fft<N, true, true>(v, buf, t, tw4);
-  if (okA) {
-#pragma unroll
-    for (int m = 0; m < S::N1; ++m) {
-      *reinterpret_cast<float4*>(tile + (t + S::T * m) * kTile) =
-          make_float4(v[m].re.x, v[m].im.x, v[m].re.y, v[m].im.y);
-    }
-  }
-  block_add_double(static_cast<double>(part.x) + static_cast<double>(part.y), inv_numel, loss);
-}
-
 // Shared memory of the adjoint row pass, per line: the exchange / scratch landing line
 // (BP), the object row (OP = N + 2: a 16-byte aligned copy shifted by the row's 8-byte
 // misalignment) and the probe row (N); per CTA: the twiddle table (N).
@@ -817,7 +711,7 @@ int check_common(const void* sample, int H, int W, const void* probe, int ph, in
     constexpr int N = decltype(NT)::value;
     if constexpr (N > 0) {
       const int sm = RegLaunch<N>::col_smem();
-      if (!st) st = ensure_smem((const void*)base_cols_pair<N>, ColPairCfg<N>::kSmemBytes);
+      if (!st) st = ensure_smem((const void*)cols_sweep_pair<N, false, true>, ColPairCfg<N>::kSmemBytes);
       if (!st) st = ensure_smem((const void*)base_cols_reg<kColForward, N>, sm);
       if (!st) st = ensure_smem((const void*)base_cols_reg<kColBackward, N>, sm);
     } else {
@@ -897,9 +791,10 @@ void launch_cols(const BaseGeom& g, int frame0, int nframes, const uint16_t* mea
     if constexpr (N > 0) {
       using L = RegLaunch<N>;
       if constexpr (MODE == kColSweep) {
+        // column DFT, amplitude-loss epilogue and inverse column DFT; counts fftshifted
         dim3 grid(num_tiles(g.pw), nframes);
-        base_cols_pair<N><<<grid, ColPairCfg<N>::kThreads, ColPairCfg<N>::kSmemBytes, s>>>(
-            g.scratch, g.pw, frame0, g.col.tw, measured, g.lut, grad_scale, inv_numel, loss);
+        cols_sweep_pair<N, false, true><<<grid, ColPairCfg<N>::kThreads, ColPairCfg<N>::kSmemBytes, s>>>(
+            g.scratch, g.pw, frame0, g.col.tw, measured, g.lut, 1.0f, grad_scale, inv_numel, loss);
         return;
       }
       dim3 grid(num_tiles(g.pw) * (kTile / kColsReg), nframes);

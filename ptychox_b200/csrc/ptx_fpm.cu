@@ -31,37 +31,103 @@ enum FpmMode { kFpmSweep = 0, kFpmForward = 1, kFpmBackward = 2 };
 
 __device__ __forceinline__ int wrap2(long long v, int n) { return static_cast<int>(v & (long long)(n - 1)); }
 
+// Shared memory of the FPM row passes, per line: the exchange / landing line (BP) and
+// two rows of N values (the gathered spectrum window row and the pupil row); per CTA the
+// twiddle table laid out by thread.
 template <int NW>
-__global__ void __launch_bounds__(256, 2) fpm_rows_forward(
+struct FpmRowCfg {
+  static constexpr int BP = RowPass<NW>::LP > NW ? RowPass<NW>::LP : NW;
+  static int smem(int lines) { return (lines * (BP + 2 * NW) + NW) * (int)sizeof(float2); }
+};
+
+// Forward row pass: gather the sub-aperture window of the spectrum (wrapping), multiply by
+// the pupil, inverse row DFT, store tiled.  Work units are (row group, frame) pairs in
+// row-group-major order over one wave of resident CTAs (CTA b takes the contiguous units
+// [u0, u1)); the pupil rows of the current row group and the twiddle table sit in shared
+// memory, and the next unit's window row is requested by cp.async (evict-last in L2: the
+// spectrum is re-read by every LED) as soon as this unit's transform has released the
+// line buffer, so it lands while this unit stores.
+template <int NW>
+__global__ void __launch_bounds__(128, 3) fpm_rows_forward(
     const float2* __restrict__ spec, int oh, int ow, const float2* __restrict__ pupil, int lh,
-    const int64_t* __restrict__ led, float2* __restrict__ scratch, const float2* __restrict__ tw, int lines) {
+    const int64_t* __restrict__ led, int nframes, int rowgroups, float2* __restrict__ scratch,
+    const float2* __restrict__ tw, int lines) {
   using S = RegShape<NW>;
+  using Cfg = FpmRowCfg<NW>;
   constexpr int kTiles = (NW + kTile - 1) / kTile;
   extern __shared__ float2 sm[];
   const int tid = threadIdx.x;
   const int l = tid / S::T;
   const int t = tid - l * S::T;
-  const int i = blockIdx.x * lines + l;  // row of G = fftshift(sub * pupil)
-  const int f = blockIdx.y;
-  const bool row_ok = i < lh;
-  const long long lx = led[2 * f], ly = led[2 * f + 1];
-  const int r = (i + lh / 2) & (lh - 1);  // window row of that G row
-  const float2* srow = spec + (size_t)wrap2(ly + r + oh / 2, oh) * ow;
-  const float2* prow = pupil + (size_t)r * NW;
-  float2 v[S::N1];
+  const long long units = (long long)rowgroups * nframes;
+  const long long u0 = units * blockIdx.x / gridDim.x;
+  const long long u1 = units * (blockIdx.x + 1) / gridDim.x;
+  if (u0 >= u1) return;
+  int g = static_cast<int>(u0 / nframes);
+  int f = static_cast<int>(u0 - (long long)g * nframes);
+  float2* buf = sm + l * Cfg::BP;
+  float2* pbuf = sm + lines * Cfg::BP + l * NW;
+  float2* tws = sm + lines * (Cfg::BP + 2 * NW);
+  load_twiddles_by_thread<NW>(tws, tw);
+  __syncthreads();
+  const uint64_t pol_last = policy_evict_last();
+  // window row of G row i (= fftshift(sub * pupil)) of `frame` into buf[t + T j]
+  auto request = [&](int i, int frame) -> bool {
+    if (i >= lh) return false;
+    const long long lx = led[2 * frame], ly = led[2 * frame + 1];
+    const int r = (i + lh / 2) & (lh - 1);
+    const float2* srow = spec + (size_t)wrap2(ly + r + oh / 2, oh) * ow;
 #pragma unroll
-  for (int j = 0; j < S::N1; ++j) {
-    const int c = (t + S::T * j + NW / 2) & (NW - 1);
-    v[j] = row_ok ? cmul(srow[wrap2(lx + c + ow / 2, ow)], __ldg(&prow[c])) : make_float2(0.f, 0.f);
-  }
-  reg_fft<NW, true, false>(v, sm + l * RowPass<NW>::LP, t, tw);
-  if (row_ok) {
-    float2* base = scratch + (size_t)f * kTiles * lh * kTile + (size_t)i * kTile;
-#pragma unroll
-    for (int m = 0; m < S::N1; ++m) {
-      const int kc = t + S::T * m;
-      base[(size_t)(kc / kTile) * lh * kTile + (kc % kTile)] = v[m];
+    for (int j = 0; j < S::N1; ++j) {
+      const int c = (t + S::T * j + NW / 2) & (NW - 1);
+      cp_async8_hint(buf + t + S::T * j, srow + wrap2(lx + c + ow / 2, ow), pol_last);
     }
+    cp_async_commit();
+    return true;
+  };
+  int i = g * lines + l;
+  bool have = request(i, f);
+  bool new_group = true;
+  for (long long u = u0; u < u1; ++u) {
+    const bool row_ok = i < lh;
+    if (new_group && row_ok) {
+      const int r = (i + lh / 2) & (lh - 1);
+#pragma unroll
+      for (int j = 0; j < S::N1; ++j) {
+        const int c = (t + S::T * j + NW / 2) & (NW - 1);
+        pbuf[t + S::T * j] = __ldg(&pupil[(size_t)r * NW + c]);
+      }
+    }
+    new_group = false;
+    cp_async_wait_all();  // own copies only: thread t copied exactly the elements it reads
+    float2 v[S::N1];
+#pragma unroll
+    for (int j = 0; j < S::N1; ++j) {
+      v[j] = have ? cmul(buf[t + S::T * j], pbuf[t + S::T * j]) : make_float2(0.f, 0.f);
+    }
+    __syncwarp();
+    reg_fft<NW, true, false, true>(v, buf, t, tws);
+    const bool more = u + 1 < u1;
+    int gn = g, fn = f + 1;
+    if (fn == nframes) {
+      gn = g + 1;
+      fn = 0;
+    }
+    const int in = gn * lines + l;
+    const bool have_next = more ? request(in, fn) : false;
+    if (row_ok) {
+      float2* base = scratch + (size_t)f * kTiles * lh * kTile + (size_t)i * kTile;
+#pragma unroll
+      for (int m = 0; m < S::N1; ++m) {
+        const int kc = t + S::T * m;
+        base[(size_t)(kc / kTile) * lh * kTile + (kc % kTile)] = v[m];
+      }
+    }
+    if (gn != g) new_group = true;
+    g = gn;
+    f = fn;
+    i = in;
+    have = have_next;
   }
 }
 
@@ -178,8 +244,15 @@ __global__ void __launch_bounds__(128, 3) fpm_rows_adjoint(
   if (u0 >= u1) return;
   int g = static_cast<int>(u0 / nframes);
   int f = static_cast<int>(u0 - (long long)g * nframes);
-  float2* buf = sm + l * RowPass<NW>::LP;
-  float2* sbuf = sm + lines * RowPass<NW>::LP + l * NW;  // prefetched window row of S
+  using Cfg = FpmRowCfg<NW>;
+  float2* buf = sm + l * Cfg::BP;
+  float2* sbuf = sm + lines * Cfg::BP + l * NW;  // prefetched window row of S
+  float2* pbuf = sm + lines * (Cfg::BP + NW) + l * NW;  // pupil row of the current row group
+  float2* tws = sm + lines * (Cfg::BP + 2 * NW);
+  load_twiddles_by_thread<NW>(tws, tw);
+  __syncthreads();
+  const uint64_t pol_last = policy_evict_last();
+  bool new_group = true;
   float2 acc[S::N1];
 #pragma unroll
   for (int m = 0; m < S::N1; ++m) acc[m] = make_float2(0.f, 0.f);
@@ -194,10 +267,18 @@ __global__ void __launch_bounds__(128, 3) fpm_rows_adjoint(
       for (int m = 0; m < S::N1; ++m) {
         const int jj = t + S::T * m;
         const int c = (jj + NW / 2) & (NW - 1);
-        cp_async8(sbuf + jj, spec + srow + wrap2(lx + c + ow / 2, ow));
+        cp_async8_hint(sbuf + jj, spec + srow + wrap2(lx + c + ow / 2, ow), pol_last);
       }
       cp_async_commit();
+      if (new_group) {
+#pragma unroll
+        for (int m = 0; m < S::N1; ++m) {
+          const int c = (t + S::T * m + NW / 2) & (NW - 1);
+          pbuf[t + S::T * m] = __ldg(&pupil[(size_t)r * NW + c]);
+        }
+      }
     }
+    new_group = false;
     float2 v[S::N1];
     if (row_ok) {
       const float2* base = scratch + (size_t)f * kTiles * lh * kTile + (size_t)i * kTile;
@@ -210,16 +291,15 @@ __global__ void __launch_bounds__(128, 3) fpm_rows_adjoint(
 #pragma unroll
       for (int j = 0; j < S::N1; ++j) v[j] = make_float2(0.f, 0.f);
     }
-    reg_fft<NW, false, false>(v, buf, t, tw);
+    reg_fft<NW, false, false, true>(v, buf, t, tws);
     if (row_ok) {
-      const float2* prow = pupil + (size_t)r * NW;
       cp_async_wait_all();
 #pragma unroll
       for (int m = 0; m < S::N1; ++m) {
         const int jj = t + S::T * m;
         const int c = (jj + NW / 2) & (NW - 1);
         const float2 gl = cscale(v[m], norm);
-        atomicAdd(&grad_spec[srow + wrap2(lx + c + ow / 2, ow)], cmulc(gl, __ldg(&prow[c])));
+        atomicAdd(&grad_spec[srow + wrap2(lx + c + ow / 2, ow)], cmulc(gl, pbuf[jj]));
         acc[m] = cadd(acc[m], cmulc(gl, sbuf[jj]));
       }
     }
@@ -229,6 +309,7 @@ __global__ void __launch_bounds__(128, 3) fpm_rows_adjoint(
       fn = 0;
     }
     if (u + 1 == u1 || gn != g) {
+      new_group = true;
       // leaving this row group: fold its pupil-gradient partial sums into grad_pupil
       if (row_ok) {
 #pragma unroll
@@ -313,12 +394,12 @@ int fpm_check(const void* object, int oh, int ow, const void* pupil, int lh, int
   });
   dispatch_pow2(lw, [&](auto NT) {
     constexpr int N = decltype(NT)::value;
-    if (!st) st = ensure_smem((const void*)fpm_rows_forward<N>, RowPass<N>::smem(RowPass<N>::lines(256, lh)));
-    if (!st) st = ensure_smem((const void*)fpm_rows_adjoint<N>, RowPass<N>::smem_with_row(RowPass<N>::lines(128, lh)));
+    if (!st) st = ensure_smem((const void*)fpm_rows_forward<N>, FpmRowCfg<N>::smem(RowPass<N>::lines(128, lh)));
+    if (!st) st = ensure_smem((const void*)fpm_rows_adjoint<N>, FpmRowCfg<N>::smem(RowPass<N>::lines(128, lh)));
   });
   dispatch_pow2(lh, [&](auto NT) {
     constexpr int N = decltype(NT)::value;
-    if (!st) st = ensure_smem((const void*)fpm_cols<kFpmSweep, N>, ColPass<N>::kSmemBytes);
+    if (!st) st = ensure_smem((const void*)cols_sweep_pair<N, true, false>, ColPairCfg<N>::kSmemBytes);
     if (!st) st = ensure_smem((const void*)fpm_cols<kFpmForward, N>, ColPass<N>::kSmemBytes);
     if (!st) st = ensure_smem((const void*)fpm_cols<kFpmBackward, N>, ColPass<N>::kSmemBytes);
   });
@@ -352,10 +433,13 @@ void launch_rows_forward(const FpmGeom& g, const float2* spec, const float2* pup
   prof_begin(kFpmRowsForward, s);
   dispatch_pow2(g.lw, [&](auto NT) {
     constexpr int N = decltype(NT)::value;
-    const int lines = RowPass<N>::lines(256, g.lh);
-    dim3 grid((g.lh + lines - 1) / lines, nf);
-    fpm_rows_forward<N><<<grid, lines * RowPass<N>::T, RowPass<N>::smem(lines), s>>>(
-        spec, g.oh, g.ow, pupil, g.lh, led, g.frames, g.p_lw.tw, lines);
+    const int lines = RowPass<N>::lines(128, g.lh);
+    const int rowgroups = (g.lh + lines - 1) / lines;
+    const int threads = lines * RowPass<N>::T, smem = FpmRowCfg<N>::smem(lines);
+    const int grid = static_cast<int>(std::min<long long>(
+        (long long)rowgroups * nf, resident_ctas((const void*)fpm_rows_forward<N>, threads, smem)));
+    fpm_rows_forward<N><<<grid, threads, smem, s>>>(spec, g.oh, g.ow, pupil, g.lh, led, nf, rowgroups, g.frames,
+                                                    g.p_lw.tw, lines);
   });
   prof_end(kFpmRowsForward, s);
 }
@@ -368,6 +452,13 @@ void launch_cols(const FpmGeom& g, int frame0, int nf, const uint16_t* measured,
   prof_begin(kFpmCols, s);
   dispatch_pow2(g.lh, [&](auto NT) {
     constexpr int N = decltype(NT)::value;
+    if constexpr (MODE == kFpmSweep) {
+      // inverse column DFT, 1/(h w), amplitude-loss epilogue, forward column DFT
+      dim3 grid(num_tiles(g.lw), nf);
+      cols_sweep_pair<N, true, false><<<grid, ColPairCfg<N>::kThreads, ColPairCfg<N>::kSmemBytes, s>>>(
+          g.frames, g.lw, frame0, g.p_lh.tw, measured, g.lut, norm, grad_scale, inv_numel, loss);
+      return;
+    }
     dim3 grid(num_tiles(g.lw) * (kTile / kColsPerCta), nf);
     fpm_cols<MODE, N><<<grid, ColPass<N>::kThreads, ColPass<N>::kSmemBytes, s>>>(
         g.frames, g.lw, frame0, g.p_lh.tw, measured, g.lut, norm, grad_scale, inv_numel, loss, image, amplitude,
@@ -384,7 +475,7 @@ void launch_rows_adjoint(const FpmGeom& g, const float2* spec, const float2* pup
     constexpr int N = decltype(NT)::value;
     const int lines = RowPass<N>::lines(128, g.lh);
     const int rowgroups = (g.lh + lines - 1) / lines;
-    const int threads = lines * RowPass<N>::T, smem = RowPass<N>::smem_with_row(lines);
+    const int threads = lines * RowPass<N>::T, smem = FpmRowCfg<N>::smem(lines);
     const int grid = static_cast<int>(std::min<long long>(
         (long long)rowgroups * nf, resident_ctas((const void*)fpm_rows_adjoint<N>, threads, smem)));
     fpm_rows_adjoint<N><<<grid, threads, smem, s>>>(g.frames, spec, g.oh, g.ow, pupil, g.lh, led, nf, rowgroups,

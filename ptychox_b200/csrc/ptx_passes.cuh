@@ -179,4 +179,117 @@ __global__ void __launch_bounds__(256, 2) fft2_cols_kernel(const float2* __restr
   }
 }
 
+// ---- column pass of a fused sweep on the two-line packed-FP32x2 FFT ------------------
+// A CTA owns one 16-column tile of one frame of the tiled scratch [frame][tile][row][16];
+// thread (p, t) transforms the column pair (2p, 2p+1) of the tile, both columns in
+// lock-step (ptx_pairfft.cuh), so every butterfly, twiddle product and epilogue operation is
+// one packed instruction for two columns.  A column pair is one 16-byte load / store per
+// row (a warp covers four whole 128-byte tile rows).  The sequence per column: DFT in the
+// FIRST_INV direction, scale by `norm`, amplitude-loss epilogue against the counts
+// (decoded through `lut`; SHIFTED: the counts are stored fftshifted in both axes), the
+// DFT in the other direction, store in place.  The tile's counts arrive by cp.async while
+// the first transform runs; the twiddle table sits in shared memory as broadcast pairs.
+template <int N>
+struct ColPairCfg {
+  static constexpr int kPairs = kTile / 2;
+  static constexpr int LP4 = RegShape<N>::BUF + 1;  // odd float4 pitch: quarter-warps conflict-free
+  static constexpr int kThreads = kPairs * RegShape<N>::T;
+  static constexpr int kExchBytes = kPairs * LP4 * (int)sizeof(float4);
+  static constexpr int kTwBytes = N * (int)sizeof(float4);
+  static constexpr int kMeasBytes = N * kTile * (int)sizeof(uint16_t);
+  static constexpr int kSmemBytes = kExchBytes + kTwBytes + kMeasBytes;
+};
+
+template <int N, bool FIRST_INV, bool SHIFTED>
+__global__ void __launch_bounds__(ColPairCfg<N>::kThreads, ColPairCfg<N>::kThreads <= 128 ? 2 : 1) cols_sweep_pair(
+    float2* __restrict__ scratch, int width, int frame0, const float2* __restrict__ tw,
+    const uint16_t* __restrict__ measured, const float* __restrict__ lut, float norm, float grad_scale,
+    double inv_numel, double* __restrict__ loss) {
+  using S = RegShape<N>;
+  using Cfg = ColPairCfg<N>;
+  extern __shared__ float4 sm4[];
+  float4* tw4 = sm4 + Cfg::kPairs * Cfg::LP4;
+  uint16_t* meas_s = reinterpret_cast<uint16_t*>(tw4 + N);
+  const int tid = threadIdx.x;
+  const int p = tid % Cfg::kPairs;
+  const int t = tid / Cfg::kPairs;
+  const int ct = blockIdx.x;
+  const int f = blockIdx.y;
+  const int c0 = ct * kTile;
+  const bool okA = c0 + 2 * p < width;
+  const bool okB = c0 + 2 * p + 1 < width;
+  float2* tile = scratch + ((size_t)f * num_tiles(width) + ct) * N * kTile + 2 * p;
+  const size_t g = (size_t)frame0 + f;
+  float4* buf = sm4 + p * Cfg::LP4;
+  constexpr int kRowOff = SHIFTED ? N / 2 : 0;
+  const int col_off = SHIFTED ? width / 2 : 0;
+
+  // counts of rows kr of the tile -> meas_s[kr][16]
+  int ic0 = c0 + col_off;
+  if (ic0 >= width) ic0 -= width;
+  const bool fast = (width % (2 * kTile) == 0) && ((reinterpret_cast<uintptr_t>(measured) & 15) == 0);
+  if (fast) {
+    for (int i = tid; i < 2 * N; i += blockDim.x) {
+      const int kr = i >> 1, h = (i & 1) * 8;
+      const int ir = (kr + kRowOff) & (N - 1);
+      cp_async16(meas_s + kr * kTile + h, measured + (g * N + ir) * width + ic0 + h);
+    }
+    cp_async_commit();
+  } else {
+    for (int i = tid; i < N * kTile; i += blockDim.x) {
+      const int kr = i / kTile, cc = i - kr * kTile;
+      const int ir = (kr + kRowOff) & (N - 1);
+      int icc = c0 + cc + col_off;
+      if (icc >= width) icc -= width;
+      meas_s[i] = (c0 + cc < width) ? measured[(g * N + ir) * width + icc] : 0;
+    }
+  }
+  for (int i = tid; i < N; i += blockDim.x) {
+    const float2 w = __ldg(&tw[i]);
+    tw4[i] = make_float4(w.x, w.x, w.y, w.y);
+  }
+  const uint64_t pol = policy_evict_first();
+  CPair v[S::N1];
+#pragma unroll
+  for (int j = 0; j < S::N1; ++j) {
+    float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (okA) q = ld_stream4(tile + (t + S::T * j) * kTile, pol);
+    if (!okB) q.z = q.w = 0.f;
+    v[j] = {make_float2(q.x, q.z), make_float2(q.y, q.w)};
+  }
+  __syncthreads();  // twiddle table
+  pair_fft<N, FIRST_INV, true>(v, buf, t, tw4);
+  cp_async_wait_all();
+  __syncthreads();
+  float2 part = make_float2(0.f, 0.f);  // squared residuals of the two columns
+  const float2 gs = f2(grad_scale);
+  const float2 nrm = f2(norm);
+#pragma unroll
+  for (int m = 0; m < S::N1; ++m) {
+    const int kr = t + S::T * m;
+    const CPair F = {mul2(v[m].re, nrm), mul2(v[m].im, nrm)};
+    const float2 s2 = fma2(F.re, F.re, mul2(F.im, F.im));
+    const float2 r = make_float2(rsqrt_nr(fmaxf(s2.x, 1e-37f)), rsqrt_nr(fmaxf(s2.y, 1e-37f)));
+    const float2 a = mul2(s2, r);
+    const float2 inv =
+        make_float2(a.x >= kEpsF32 ? r.x : 1.0f / kEpsF32, a.y >= kEpsF32 ? r.y : 1.0f / kEpsF32);
+    const uint32_t cnt = *reinterpret_cast<const uint32_t*>(meas_s + kr * kTile + 2 * p);
+    const float2 y = make_float2(okA ? __ldg(&lut[cnt & 0xffffu]) : 0.f, okB ? __ldg(&lut[cnt >> 16]) : 0.f);
+    float2 rr = sub2(a, y);
+    rr = make_float2(okA ? rr.x : 0.f, okB ? rr.y : 0.f);
+    part = fma2(rr, rr, part);
+    const float2 sc = mul2(mul2(gs, rr), inv);
+    v[m] = {mul2(F.re, sc), mul2(F.im, sc)};
+  }
+  pair_fft<N, !FIRST_INV, true>(v, buf, t, tw4);
+  if (okA) {
+#pragma unroll
+    for (int m = 0; m < S::N1; ++m) {
+      *reinterpret_cast<float4*>(tile + (t + S::T * m) * kTile) =
+          make_float4(v[m].re.x, v[m].im.x, v[m].re.y, v[m].im.y);
+    }
+  }
+  block_add_double(static_cast<double>(part.x) + static_cast<double>(part.y), inv_numel, loss);
+}
+
 }  // namespace ptx
