@@ -373,6 +373,42 @@ class ClockSampler:
 # ---------------------------------------------------------------------------------------
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of all kernels of one sweep, from
+# the ncu captures summarised in profiles/ (the same scope as `achieved`: one whole sweep).
+MEASURED_TRAFFIC = {
+    "conventional-900x512-2048": (7.319e9, "profiles/base_sweep_kernels_96positions_full.md",
+                                  "96-position capture scaled by 900/96"),
+    "fourier-225x256-1024": (0.4376e9, "profiles/fpm_sweep_225x256_full.md", "full-size capture"),
+    "coded-64x1024-ds4": (7.10e9, "profiles/coded_sweep_16x1024_full.md", "16-shift capture scaled by 64/16"),
+}
+
+
+def subset(wl: Workload, k: int) -> Workload:
+    """The same workload on its first k scan units (positions, LEDs or shifts), for small
+    profiling cases; the JSON line records the subset in its config."""
+    import copy
+
+    w = copy.copy(wl)
+    full_host = wl.host
+
+    def host(seed):
+        h = full_host(seed)
+        h["pos"] = h["pos"][:k]
+        return h
+
+    w.host = host
+    w.batch = min(k, wl.batch)
+    full_config = wl.config
+
+    def config():
+        c = full_config()
+        c["units_subset"] = w.batch
+        return c
+
+    w.config = config
+    return w
+
+
 def run_ours(args) -> None:
     import torch
     import torch.distributed as dist
@@ -380,6 +416,8 @@ def run_ours(args) -> None:
     from ptychox_b200 import _abi
 
     wl = WORKLOADS[args.workload]
+    if args.units:
+        wl = subset(wl, args.units)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -464,7 +502,8 @@ def run_ours(args) -> None:
         "peak": peak,
         "unit": "GB/s",
         "frac": achieved / peak,
-        "traffic": None,
+        "traffic": None if args.units else MEASURED_TRAFFIC.get(wl.name, (None,))[0],
+        "traffic_source": None if args.units else MEASURED_TRAFFIC.get(wl.name, (None, None, None))[1:],
         "peak_kind": f"{peak_kind} hbm_gbs (of {peak_kind})",
         "scope": "fused sweep: all passes of one sweep on one stream, algorithmic bytes per sweep / sweep time",
         "algorithmic_bytes_per_sweep": sweep_bytes,
@@ -736,6 +775,8 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
+    ap.add_argument("--units", type=int, default=0,
+                    help="run the workload on its first N scan units only (small profiling cases)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
