@@ -718,7 +718,8 @@ def run_serving(args) -> None:
     clocks.start()
     launches0 = _abi.query("ptx_launch_count")
     t0 = time.perf_counter()
-    served = ReconstructionServer(dev, max_active=args.max_active).run(reqs, realtime=True)
+    served = ReconstructionServer(dev, max_active=args.max_active, units_per_cta=args.units_per_cta).run(
+        reqs, realtime=True)
     t_served = time.perf_counter() - t0
     launches = _abi.query("ptx_launch_count") - launches0
     clk = clocks.stop()
@@ -772,6 +773,8 @@ def main() -> None:
     ap.add_argument("--requests", type=int, default=40)
     ap.add_argument("--iters", type=int, default=50)
     ap.add_argument("--max-active", type=int, default=8)
+    ap.add_argument("--units-per-cta", type=int, default=8,
+                    help="serving: bound on the units a persistent-pass CTA takes (0: one wave)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=12.0)

@@ -56,6 +56,15 @@ int ptx_clear_cache(void);
 /* Number of kernels this library has launched in the process (all devices). */
 long long ptx_launch_count(void);
 
+/* Work granularity of the persistent row passes (process-wide, default 0).  0: each such
+ * pass runs one wave of resident CTAs, every CTA taking an equal share of the (row group,
+ * frame) units -- the fastest layout when one sweep has the GPU to itself.  k > 0: enough
+ * CTAs that none takes more than k units, so kernels that other streams launch meanwhile
+ * (several reconstructions served at once) interleave with the pass CTA by CTA.  Applies to
+ * launches made (or captured into CUDA graphs) after the call.  No reference counterpart:
+ * the reference's kernels are one-shot grids. */
+int ptx_set_units_per_cta(int units);
+
 /* Optional per-kernel CUDA-event timing: when enabled every launch is bracketed by an
  * event pair on its stream.  ptx_profile_read synchronises on the recorded events and
  * returns the accumulated device time and timed launches of one kernel kind

@@ -740,8 +740,7 @@ void launch_rows_forward(const BaseGeom& g, const float2* sample, const float2* 
       const int lines = L::lines(128, g.ph);
       const int rowgroups = (g.ph + lines - 1) / lines;
       const int threads = lines * L::T, smem = FwdCfg<N>::smem(lines);
-      const int grid = static_cast<int>(std::min<long long>(
-          (long long)rowgroups * nframes, resident_ctas((const void*)base_rows_forward_reg<N>, threads, smem)));
+      const int grid = persistent_grid((const void*)base_rows_forward_reg<N>, threads, smem, (long long)rowgroups * nframes);
       base_rows_forward_reg<N><<<grid, threads, smem, s>>>(sample, g.H, g.W, probe, g.ph, pos, nframes, rowgroups,
                                                            g.scratch, g.row.tw, lines, g.err);
     } else {
@@ -765,8 +764,7 @@ void launch_rows_adjoint(const BaseGeom& g, const float2* sample, const float2* 
       const int rowgroups = (g.ph + lines - 1) / lines;
       const int threads = lines * L::T, smem = L::adj_smem(lines);
       const long long units = (long long)rowgroups * nframes;
-      const int grid = static_cast<int>(
-          std::min<long long>(units, resident_ctas((const void*)base_rows_adjoint_reg<N>, threads, smem)));
+      const int grid = persistent_grid((const void*)base_rows_adjoint_reg<N>, threads, smem, units);
       base_rows_adjoint_reg<N><<<grid, threads, smem, s>>>(g.scratch, sample, g.H, g.W, probe, g.ph, pos, nframes,
                                                            rowgroups, grad_sample, grad_probe, g.row.tw, lines);
     } else {

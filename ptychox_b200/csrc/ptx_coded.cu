@@ -478,8 +478,7 @@ void launch_rows_grad_mask(const CodedGeom& g, int nf, const float2* mask, const
     const int lines = RowPass<N>::lines(128, N);
     const int rowgroups = (N + lines - 1) / lines;
     const int threads = lines * RowPass<N>::T, smem = RowPass<N>::smem_with_row(lines);
-    const int grid = static_cast<int>(std::min<long long>(
-        (long long)rowgroups * nf, resident_ctas((const void*)coded_rows_grad_mask<N>, threads, smem)));
+    const int grid = persistent_grid((const void*)coded_rows_grad_mask<N>, threads, smem, (long long)rowgroups * nf);
     coded_rows_grad_mask<N><<<grid, threads, smem, s>>>(g.frames, mask, xstore, nf, rowgroups, grad_mask, g.plan.tw,
                                                         lines);
   });

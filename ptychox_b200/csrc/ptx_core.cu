@@ -257,9 +257,24 @@ int resident_ctas(const void* kernel, int threads, int smem) {
   return n;
 }
 
+std::atomic<int> g_units_per_cta{0};
+
+int persistent_grid(const void* kernel, int threads, int smem, long long units) {
+  long long grid = std::min<long long>(units, resident_ctas(kernel, threads, smem));
+  const int k = g_units_per_cta.load(std::memory_order_relaxed);
+  if (k > 0) grid = std::max(grid, (units + k - 1) / k);
+  return static_cast<int>(std::max<long long>(1, std::min<long long>(grid, std::max<long long>(units, 1))));
+}
+
 }  // namespace ptx
 
 extern "C" {
+
+int ptx_set_units_per_cta(int units) {
+  if (units < 0) return ptx::set_error(PTX_ERR_INVALID_ARGUMENT, "units per CTA must be >= 0");
+  ptx::g_units_per_cta.store(units, std::memory_order_relaxed);
+  return PTX_OK;
+}
 
 int ptx_version(void) { return 100; }  // 0.1.0
 

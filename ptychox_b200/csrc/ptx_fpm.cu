@@ -436,8 +436,7 @@ void launch_rows_forward(const FpmGeom& g, const float2* spec, const float2* pup
     const int lines = RowPass<N>::lines(128, g.lh);
     const int rowgroups = (g.lh + lines - 1) / lines;
     const int threads = lines * RowPass<N>::T, smem = FpmRowCfg<N>::smem(lines);
-    const int grid = static_cast<int>(std::min<long long>(
-        (long long)rowgroups * nf, resident_ctas((const void*)fpm_rows_forward<N>, threads, smem)));
+    const int grid = persistent_grid((const void*)fpm_rows_forward<N>, threads, smem, (long long)rowgroups * nf);
     fpm_rows_forward<N><<<grid, threads, smem, s>>>(spec, g.oh, g.ow, pupil, g.lh, led, nf, rowgroups, g.frames,
                                                     g.p_lw.tw, lines);
   });
@@ -476,8 +475,7 @@ void launch_rows_adjoint(const FpmGeom& g, const float2* spec, const float2* pup
     const int lines = RowPass<N>::lines(128, g.lh);
     const int rowgroups = (g.lh + lines - 1) / lines;
     const int threads = lines * RowPass<N>::T, smem = FpmRowCfg<N>::smem(lines);
-    const int grid = static_cast<int>(std::min<long long>(
-        (long long)rowgroups * nf, resident_ctas((const void*)fpm_rows_adjoint<N>, threads, smem)));
+    const int grid = persistent_grid((const void*)fpm_rows_adjoint<N>, threads, smem, (long long)rowgroups * nf);
     fpm_rows_adjoint<N><<<grid, threads, smem, s>>>(g.frames, spec, g.oh, g.ow, pupil, g.lh, led, nf, rowgroups,
                                                     norm, grad_spec, grad_pupil, g.p_lw.tw, lines);
   });

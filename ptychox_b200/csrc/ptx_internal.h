@@ -50,6 +50,10 @@ int sm_count();
 // (device, kernel, threads, smem).
 int resident_ctas(const void* kernel, int threads, int smem);
 
+// Grid of a persistent pass over `units` work units: one wave of resident CTAs, or, when
+// ptx_set_units_per_cta(k > 0) is in force, enough CTAs that none takes more than k units.
+int persistent_grid(const void* kernel, int threads, int smem, long long units);
+
 // Kernel kinds for the launch counter and the optional per-kernel event profiler.
 enum KernelId {
   kBaseRowsForward = 0,

@@ -205,7 +205,7 @@ class ReconstructionServer:
 
     def __init__(self, device: torch.device | str = "cuda", hbm_budget: int | None = None,
                  max_active: int = 8, workspace_cap: int = 512 << 20, use_graphs: bool = True,
-                 max_inflight: int = 2):
+                 max_inflight: int = 2, units_per_cta: int = 8):
         self.dev = torch.device(device)
         if hbm_budget is None:
             free, _ = torch.cuda.mem_get_info(self.dev)
@@ -215,10 +215,19 @@ class ReconstructionServer:
         self.ws_cap = int(workspace_cap)
         self.use_graphs = use_graphs
         self.max_inflight = max_inflight
+        # persistent passes of concurrent reconstructions must interleave CTA by CTA
+        self.units_per_cta = int(units_per_cta)
 
     def run(self, requests: list[ReconRequest], realtime: bool = True) -> list[ReconResult]:
         """Serve ``requests`` (arrival times in seconds from the start); returns results in rid order."""
         _abi.load()
+        _abi.query("ptx_set_units_per_cta", self.units_per_cta)
+        try:
+            return self._run(requests, realtime)
+        finally:
+            _abi.query("ptx_set_units_per_cta", 0)
+
+    def _run(self, requests: list[ReconRequest], realtime: bool) -> list[ReconResult]:
         pending = sorted(requests, key=lambda r: (r.arrival, r.rid))
         for r in pending:
             if request_bytes(r, self.ws_cap) > self.budget:

@@ -52,6 +52,10 @@ def test_pure_host_entry_points(lib):
     assert ws >= hdr + frame and (ws - hdr) % frame == 0
     assert lib.ptx_base_workspace_bytes(128, 128, 3) == hdr + 3 * 128 * 128 * 8
     assert lib.ptx_base_workspace_bytes(0, 16, 1) == 0
+    # persistent-pass granularity knob: a host-side setting, negative values rejected
+    assert lib.ptx_set_units_per_cta(4) == 0
+    assert lib.ptx_set_units_per_cta(-1) != 0
+    assert lib.ptx_set_units_per_cta(0) == 0
 
 
 def test_reference_input_checks_and_messages():
