@@ -182,8 +182,8 @@ int ptx_coded_forward(const float* object, const float* coded_surface,
                       float* x_forward, float* sensor, float* amplitude,
                       void* workspace, size_t workspace_bytes, void* stream);
 
-/* Adjoint for grad_output (float32 [batch, n/ds, n/ds]) from the saved forward arrays;
- * grad_object and grad_coded (complex64 [n, n]) are OVERWRITTEN.
+/* Adjoint for grad_output (float32 [batch, n/ds, n/ds]) from the saved forward arrays
+ * (x_forward 16-byte aligned); grad_object and grad_coded (complex64 [n, n]) are OVERWRITTEN.
  * Replaces coded_kernel.cu:347-424. */
 int ptx_coded_backward(const float* grad_output, const float* x_forward, const float* sensor,
                        const float* amplitude, const float* coded_surface,

@@ -140,6 +140,38 @@ __device__ __forceinline__ void load_frame_row(const float2* __restrict__ scratc
   }
 }
 
+// Frame row r of frame f loaded straight into registers with loads that do not allocate in
+// L1 (the frames stream through once per pass; L1 is left to the twiddles and masks).
+template <int N>
+__device__ __forceinline__ void load_frame_row_stream(const float2* __restrict__ scratch, int f, int r,
+                                                      float2 (&v)[RegShape<N>::N1], int t, uint64_t pol) {
+  using S = RegShape<N>;
+  constexpr int kTiles = (N + kTile - 1) / kTile;
+  const float2* base = scratch + (size_t)f * kTiles * N * kTile + (size_t)r * kTile;
+#pragma unroll
+  for (int j = 0; j < S::N1; ++j) {
+    const int c = t + S::T * j;
+    const float4 q = ld_stream4(base + (size_t)(c / kTile) * N * kTile + (c % kTile) - (c & 1), pol);
+    v[j] = (c & 1) ? make_float2(q.z, q.w) : make_float2(q.x, q.y);
+  }
+}
+// Frame row r of frame f into the line buffer `dst` (element c at dst[c]) by 16-byte
+// cp.async that bypasses L1; thread t of the line's T threads copies chunks t + T i, so the
+// line meets at a warp barrier after the wait before reading.
+template <int N>
+__device__ __forceinline__ void prefetch_frame_row(float2* dst, const float2* __restrict__ scratch, int f, int r,
+                                                   int t, uint64_t pol) {
+  using S = RegShape<N>;
+  constexpr int kTiles = (N + kTile - 1) / kTile;
+  const float2* base = scratch + (size_t)f * kTiles * N * kTile + (size_t)r * kTile;
+#pragma unroll
+  for (int i = 0; i < S::N1 / 2; ++i) {
+    const int c = 2 * (t + S::T * i);
+    cp_async16_hint(dst + c, base + (size_t)(c / kTile) * N * kTile + (c % kTile), pol);
+  }
+  cp_async_commit();
+}
+
 template <int N>
 __device__ __forceinline__ void store_frame_row(float2* __restrict__ scratch, int f, int r,
                                                 const float2 (&v)[RegShape<N>::N1], int t) {
@@ -153,35 +185,84 @@ __device__ __forceinline__ void store_frame_row(float2* __restrict__ scratch, in
   }
 }
 
-// Pass 2: inverse row DFT, x = ./n (stored), a = x M, forward row DFT.
+// Shared memory of the persistent coded row passes, per line: the exchange / landing line
+// (BP), then `rows` further rows of N values (mask row; x row); per CTA the twiddle table
+// laid out by thread.
 template <int N>
-__global__ void __launch_bounds__(256, 2) coded_rows_mask(float2* __restrict__ scratch,
+struct CodedRowCfg {
+  static constexpr int BP = RowPass<N>::LP > N ? RowPass<N>::LP : N;
+  static_assert(BP % 2 == 0, "16-byte landing lines");
+  static int smem(int lines, int rows) { return (lines * (BP + rows * N) + N) * (int)sizeof(float2); }
+};
+
+// Pass 2: inverse row DFT, x = ./n (stored), a = x M, forward row DFT.  Work units are
+// (row group, frame) pairs in row-group-major order over one wave of resident CTAs (CTA b
+// takes the contiguous units [u0, u1)); the mask rows of the current row group and the
+// twiddle table sit in shared memory, and the next unit's frame row is requested by
+// cp.async as soon as this unit's transforms have released the line buffer.
+template <int N>
+__global__ void __launch_bounds__(128, 3) coded_rows_mask(float2* __restrict__ scratch,
                                                           const float2* __restrict__ mask,
-                                                          float2* __restrict__ xstore, float inv_n,
-                                                          const float2* __restrict__ tw, int lines) {
+                                                          float2* __restrict__ xstore, float inv_n, int nframes,
+                                                          int rowgroups, const float2* __restrict__ tw, int lines) {
   using S = RegShape<N>;
+  using Cfg = CodedRowCfg<N>;
   extern __shared__ float2 sm[];
   const int tid = threadIdx.x;
   const int l = tid / S::T;
   const int t = tid - l * S::T;
-  const int r = blockIdx.x * lines + l;
-  const int f = blockIdx.y;
-  const bool row_ok = r < N;
-  const int rr = row_ok ? r : 0;
-  float2 v[S::N1];
-  load_frame_row<N>(scratch, f, rr, v, t);
-  reg_fft<N, true, false>(v, sm + l * RowPass<N>::LP, t, tw);
-  float2* xrow = xstore + ((size_t)f * N + rr) * N;
-  const float2* mrow = mask + (size_t)rr * N;
+  const long long units = (long long)rowgroups * nframes;
+  const long long u0 = units * blockIdx.x / gridDim.x;
+  const long long u1 = units * (blockIdx.x + 1) / gridDim.x;
+  if (u0 >= u1) return;
+  int g = static_cast<int>(u0 / nframes);
+  int f = static_cast<int>(u0 - (long long)g * nframes);
+  float2* buf = sm + l * Cfg::BP;
+  float2* mbuf = sm + lines * Cfg::BP + l * N;
+  float2* tws = sm + lines * (Cfg::BP + N);
+  load_twiddles_by_thread<N>(tws, tw);
+  __syncthreads();
+  const uint64_t pol_first = policy_evict_first();
+  int r = g * lines + l;
+  if (r < N) prefetch_frame_row<N>(buf, scratch, f, r, t, pol_first);
+  bool new_group = true;
+  for (long long u = u0; u < u1; ++u) {
+    const bool row_ok = r < N;
+    if (new_group && row_ok) {
 #pragma unroll
-  for (int m = 0; m < S::N1; ++m) {
-    const int c = t + S::T * m;
-    const float2 x = cscale(v[m], inv_n);
-    if (row_ok) xrow[c] = x;
-    v[m] = cmul(x, __ldg(&mrow[c]));
+      for (int m = 0; m < S::N1; ++m) mbuf[t + S::T * m] = __ldg(&mask[(size_t)r * N + t + S::T * m]);
+    }
+    new_group = false;
+    cp_async_wait_all();
+    __syncwarp();
+    float2 v[S::N1];
+#pragma unroll
+    for (int j = 0; j < S::N1; ++j) v[j] = row_ok ? buf[t + S::T * j] : make_float2(0.f, 0.f);
+    __syncwarp();
+    reg_fft<N, true, false, true>(v, buf, t, tws);
+    float2* xrow = xstore + ((size_t)f * N + (row_ok ? r : 0)) * N;
+#pragma unroll
+    for (int m = 0; m < S::N1; ++m) {
+      const int c = t + S::T * m;
+      const float2 x = cscale(v[m], inv_n);
+      if (row_ok) xrow[c] = x;
+      v[m] = cmul(x, mbuf[c]);
+    }
+    reg_fft<N, false, false, true>(v, buf, t, tws);
+    const bool more = u + 1 < u1;
+    int gn = g, fn = f + 1;
+    if (fn == nframes) {
+      gn = g + 1;
+      fn = 0;
+    }
+    const int rn = gn * lines + l;
+    if (more && rn < N) prefetch_frame_row<N>(buf, scratch, fn, rn, t, pol_first);
+    if (row_ok) store_frame_row<N>(scratch, f, r, v, t);
+    if (gn != g) new_group = true;
+    g = gn;
+    f = fn;
+    r = rn;
   }
-  reg_fft<N, false, false>(v, sm + l * RowPass<N>::LP, t, tw);
-  if (row_ok) store_frame_row<N>(scratch, f, r, v, t);
 }
 
 // Pass 4.  kCodedSweep: inverse row DFT, s = ./n, RMS pool over ds x ds, FP64 loss,
@@ -197,6 +278,9 @@ __global__ void __launch_bounds__(256, 2) coded_rows_pool(
   using S = RegShape<N>;
   extern __shared__ float2 sm[];
   float* pool = reinterpret_cast<float*>(sm + lines * RowPass<N>::LP);  // [lines][N] |s|^2, then factors
+  float2* tws = reinterpret_cast<float2*>(pool + lines * N);             // twiddles by thread
+  load_twiddles_by_thread<N>(tws, tw);
+  __syncthreads();
   const int tid = threadIdx.x;
   const int l = tid / S::T;
   const int t = tid - l * S::T;
@@ -217,8 +301,8 @@ __global__ void __launch_bounds__(256, 2) coded_rows_pool(
       v[m] = cscale(srow[c], grow[c / ds] / (a * static_cast<float>(ds * ds)));
     }
   } else {
-    load_frame_row<N>(scratch, f, r, v, t);
-    reg_fft<N, true, false>(v, sm + l * RowPass<N>::LP, t, tw);
+    load_frame_row_stream<N>(scratch, f, r, v, t, policy_evict_first());
+    reg_fft<N, true, false, true>(v, sm + l * RowPass<N>::LP, t, tws);
 #pragma unroll
     for (int m = 0; m < S::N1; ++m) {
       v[m] = cscale(v[m], inv_n);
@@ -258,14 +342,14 @@ __global__ void __launch_bounds__(256, 2) coded_rows_pool(
       v[m] = cscale(v[m], pool[((l / ds) * ds) * N + (c / ds) * ds]);
     }
   }
-  reg_fft<N, false, false>(v, sm + l * RowPass<N>::LP, t, tw);
+  reg_fft<N, false, false, true>(v, sm + l * RowPass<N>::LP, t, tws);
   store_frame_row<N>(scratch, f, r, v, t);
 }
 
 // Pass 6: inverse row DFT (g_a), grad_M += g_a conj(x) in registers over the CTA's frames,
 // g_a conj(M), forward row DFT.
 template <int N>
-__global__ void __launch_bounds__(128, 3) coded_rows_grad_mask(
+__global__ void __launch_bounds__(128, 2) coded_rows_grad_mask(
     float2* __restrict__ scratch, const float2* __restrict__ mask, const float2* __restrict__ xstore, int nframes,
     int rowgroups, float2* __restrict__ grad_mask, const float2* __restrict__ tw, int lines) {
   using S = RegShape<N>;
@@ -281,31 +365,51 @@ __global__ void __launch_bounds__(128, 3) coded_rows_grad_mask(
   if (u0 >= u1) return;
   int g = static_cast<int>(u0 / nframes);
   int f = static_cast<int>(u0 - (long long)g * nframes);
-  float2* buf = sm + l * RowPass<N>::LP;
-  float2* xbuf = sm + lines * RowPass<N>::LP + l * N;
+  using Cfg = CodedRowCfg<N>;
+  float2* buf = sm + l * Cfg::BP;
+  float2* xbuf = sm + lines * Cfg::BP + l * 2 * N;
+  float2* mbuf = xbuf + N;
+  float2* tws = sm + lines * (Cfg::BP + 2 * N);
+  load_twiddles_by_thread<N>(tws, tw);
+  __syncthreads();
+  const uint64_t pol_first = policy_evict_first();
   float2 acc[S::N1];
 #pragma unroll
   for (int m = 0; m < S::N1; ++m) acc[m] = make_float2(0.f, 0.f);
+  bool new_group = true;
   for (long long u = u0; u < u1; ++u) {
     const int r = g * lines + l;
     const bool row_ok = r < N;
     const int rr = row_ok ? r : 0;
-    const float2* mrow = mask + (size_t)rr * N;
-    const float2* xrow = xstore + ((size_t)f * N + rr) * N;
+    if (new_group && row_ok) {
 #pragma unroll
-    for (int m = 0; m < S::N1; ++m) cp_async8(xbuf + t + S::T * m, xrow + t + S::T * m);
+      for (int m = 0; m < S::N1; ++m) mbuf[t + S::T * m] = __ldg(&mask[(size_t)r * N + t + S::T * m]);
+    }
+    new_group = false;
+    const float2* xrow = xstore + ((size_t)f * N + rr) * N;
+    prefetch_frame_row<N>(buf, scratch, f, rr, t, pol_first);
+#pragma unroll
+    for (int i = 0; i < S::N1 / 2; ++i) {
+      const int c = 2 * (t + S::T * i);
+      cp_async16_hint(xbuf + c, xrow + c, pol_first);
+    }
     cp_async_commit();
+    asm volatile("cp.async.wait_group 1;\n" ::: "memory");  // the frame row
+    __syncwarp();
     float2 v[S::N1];
-    load_frame_row<N>(scratch, f, rr, v, t);
-    reg_fft<N, true, false>(v, buf, t, tw);
-    cp_async_wait_all();
+#pragma unroll
+    for (int j = 0; j < S::N1; ++j) v[j] = buf[t + S::T * j];
+    __syncwarp();
+    reg_fft<N, true, false, true>(v, buf, t, tws);
+    cp_async_wait_all();  // the x row
+    __syncwarp();
 #pragma unroll
     for (int m = 0; m < S::N1; ++m) {
       const int c = t + S::T * m;
       acc[m] = cadd(acc[m], cmulc(v[m], xbuf[c]));
-      v[m] = cmulc(v[m], __ldg(&mrow[c]));
+      v[m] = cmulc(v[m], mbuf[c]);
     }
-    reg_fft<N, false, false>(v, buf, t, tw);
+    reg_fft<N, false, false, true>(v, buf, t, tws);
     if (row_ok) store_frame_row<N>(scratch, f, r, v, t);
     int gn = g, fn = f + 1;
     if (fn == nframes) {
@@ -313,6 +417,7 @@ __global__ void __launch_bounds__(128, 3) coded_rows_grad_mask(
       fn = 0;
     }
     if (u + 1 == u1 || gn != g) {
+      new_group = true;
       // leaving this row group: fold its mask-gradient partial sums into grad_mask
       if (row_ok) {
 #pragma unroll
@@ -389,8 +494,8 @@ int coded_check(int n, int ds, const void* a, const void* b, const void* t2, con
   dispatch_pow2(n, [&](auto NT) {
     constexpr int N = decltype(NT)::value;
     const int rs = RowPass<N>::smem(lines);
-    const int rs_row = RowPass<N>::smem_with_row(RowPass<N>::lines(128, N));
-    const int pool = rs + lines * N * (int)sizeof(float);
+    const int lines128 = RowPass<N>::lines(128, N);
+    const int pool = rs + lines * N * (int)sizeof(float) + N * (int)sizeof(float2);
     const int cs = kColsPerCta * ColPass<N>::LP * (int)sizeof(float2);
     if (!st) st = ensure_smem((const void*)fft2_rows_kernel<N, false>, rs);
     if (!st) st = ensure_smem((const void*)fft2_rows_kernel<N, true>, rs);
@@ -400,11 +505,11 @@ int coded_check(int n, int ds, const void* a, const void* b, const void* t2, con
     if (!st) st = ensure_smem((const void*)coded_cols<3, false, N>, cs);
     if (!st) st = ensure_smem((const void*)coded_cols<3, true, N>, cs);
     if (!st) st = ensure_smem((const void*)coded_cols<7, false, N>, cs);
-    if (!st) st = ensure_smem((const void*)coded_rows_mask<N>, rs);
+    if (!st) st = ensure_smem((const void*)coded_rows_mask<N>, CodedRowCfg<N>::smem(lines128, 1));
     if (!st) st = ensure_smem((const void*)coded_rows_pool<kCodedSweep, N>, pool);
     if (!st) st = ensure_smem((const void*)coded_rows_pool<kCodedForward, N>, pool);
     if (!st) st = ensure_smem((const void*)coded_rows_pool<kCodedBackward, N>, pool);
-    if (!st) st = ensure_smem((const void*)coded_rows_grad_mask<N>, rs_row);
+    if (!st) st = ensure_smem((const void*)coded_rows_grad_mask<N>, CodedRowCfg<N>::smem(lines128, 2));
   });
   return st;
 }
@@ -444,10 +549,11 @@ void launch_rows_mask(const CodedGeom& g, int nf, const float2* mask, float2* xs
   prof_begin(kCodedRows, s);
   dispatch_pow2(g.n, [&](auto NT) {
     constexpr int N = decltype(NT)::value;
-    const int lines = RowPass<N>::lines(256, N);
-    dim3 grid((N + lines - 1) / lines, nf);
-    coded_rows_mask<N><<<grid, lines * RowPass<N>::T, RowPass<N>::smem(lines), s>>>(g.frames, mask, xstore, inv_n,
-                                                                                   g.plan.tw, lines);
+    const int lines = RowPass<N>::lines(128, N);
+    const int rowgroups = (N + lines - 1) / lines;
+    const int threads = lines * RowPass<N>::T, smem = CodedRowCfg<N>::smem(lines, 1);
+    const int grid = persistent_grid((const void*)coded_rows_mask<N>, threads, smem, (long long)rowgroups * nf);
+    coded_rows_mask<N><<<grid, threads, smem, s>>>(g.frames, mask, xstore, inv_n, nf, rowgroups, g.plan.tw, lines);
   });
   prof_end(kCodedRows, s);
 }
@@ -462,7 +568,7 @@ void launch_rows_pool(const CodedGeom& g, int frame0, int nf, const uint16_t* me
     constexpr int N = decltype(NT)::value;
     const int lines = RowPass<N>::lines(256, N);
     dim3 grid((N + lines - 1) / lines, nf);
-    const int smem = RowPass<N>::smem(lines) + lines * N * (int)sizeof(float);
+    const int smem = RowPass<N>::smem(lines) + lines * N * (int)sizeof(float) + N * (int)sizeof(float2);
     coded_rows_pool<MODE, N><<<grid, lines * RowPass<N>::T, smem, s>>>(g.frames, g.ds, frame0, inv_n, measured, scale,
                                                                        grad_scale, inv_numel, loss, sensor, amplitude,
                                                                        grad_output, g.plan.tw, lines);
@@ -477,7 +583,7 @@ void launch_rows_grad_mask(const CodedGeom& g, int nf, const float2* mask, const
     constexpr int N = decltype(NT)::value;
     const int lines = RowPass<N>::lines(128, N);
     const int rowgroups = (N + lines - 1) / lines;
-    const int threads = lines * RowPass<N>::T, smem = RowPass<N>::smem_with_row(lines);
+    const int threads = lines * RowPass<N>::T, smem = CodedRowCfg<N>::smem(lines, 2);
     const int grid = persistent_grid((const void*)coded_rows_grad_mask<N>, threads, smem, (long long)rowgroups * nf);
     coded_rows_grad_mask<N><<<grid, threads, smem, s>>>(g.frames, mask, xstore, nf, rowgroups, grad_mask, g.plan.tw,
                                                         lines);
@@ -544,6 +650,9 @@ int ptx_coded_backward(const float* grad_output, const float* x_forward, const f
   }
   if (((!grad_output || !x_forward || !sensor || !amplitude) && batch > 0) || !grad_object || !grad_coded) {
     return set_error(PTX_ERR_INVALID_ARGUMENT, "null pointer argument");
+  }
+  if (reinterpret_cast<uintptr_t>(x_forward) & 15) {
+    return set_error(PTX_ERR_INVALID_ARGUMENT, "x_forward must be 16-byte aligned");
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const float2* T1 = reinterpret_cast<const float2*>(transfer_1);
