@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "ptx_internal.h"
 #include "ptx_passes.cuh"
@@ -122,6 +123,58 @@ __global__ void __launch_bounds__(256, 2) coded_cols(
   if (col_ok) {
 #pragma unroll
     for (int m = 0; m < S::N1; ++m) tile[(t + S::T * m) * kTile + c] = v[m];
+  }
+}
+
+// Stage 3 on the two-line packed FFT: a CTA owns one 16-column tile of one frame; thread
+// (p, t) transforms the column pair (2p, 2p+1) in lock-step (forward DFT, x T2 or
+// conj(T2)/n, inverse DFT).  One 16-byte load / store per row and column pair.
+template <bool CONJ, int N>
+__global__ void __launch_bounds__(ColPairCfg<N>::kThreads, ColPairCfg<N>::kThreads <= 128 ? 2 : 1) coded_cols_filter_pair(
+    float2* __restrict__ scratch, const float2* __restrict__ t2, float inv_n, const float2* __restrict__ tw) {
+  using S = RegShape<N>;
+  using Cfg = ColPairCfg<N>;
+  constexpr int kTiles = (N + kTile - 1) / kTile;
+  extern __shared__ float4 sm4[];
+  float4* tw4 = sm4 + Cfg::kPairs * Cfg::LP4;
+  const int tid = threadIdx.x;
+  const int p = tid % Cfg::kPairs;
+  const int t = tid / Cfg::kPairs;
+  const int ct = blockIdx.x;
+  const int f = blockIdx.y;
+  const int c = ct * kTile + 2 * p;  // line A column (line B: c + 1; N is a multiple of 16)
+  float2* tile = scratch + ((size_t)f * kTiles + ct) * N * kTile + 2 * p;
+  float4* buf = sm4 + p * Cfg::LP4;
+  for (int i = tid; i < N; i += blockDim.x) {
+    const float2 w = __ldg(&tw[i]);
+    tw4[i] = make_float4(w.x, w.x, w.y, w.y);
+  }
+  const uint64_t pol = policy_evict_first();
+  CPair v[S::N1];
+#pragma unroll
+  for (int j = 0; j < S::N1; ++j) {
+    const float4 q = ld_stream4(tile + (t + S::T * j) * kTile, pol);
+    v[j] = {make_float2(q.x, q.z), make_float2(q.y, q.w)};
+  }
+  __syncthreads();  // twiddle table
+  pair_fft<N, false, true>(v, buf, t, tw4);
+  const float2 sc = f2(inv_n);
+#pragma unroll
+  for (int m = 0; m < S::N1; ++m) {
+    const int kr = t + S::T * m;
+    const float4 q = __ldg(reinterpret_cast<const float4*>(t2 + (size_t)kr * N + c));
+    const float2 hre = make_float2(q.x, q.z), him = make_float2(q.y, q.w);
+    const CPair a = v[m];
+    if (CONJ) {  // cscale(cmulc(a, h), inv_n)
+      v[m] = {mul2(fma2(a.re, hre, mul2(a.im, him)), sc), mul2(fma2(a.im, hre, mul2(a.re, neg2(him))), sc)};
+    } else {  // cmul(a, h)
+      v[m] = {fma2(a.re, hre, mul2(a.im, neg2(him))), fma2(a.re, him, mul2(a.im, hre))};
+    }
+  }
+  pair_fft<N, true, true>(v, buf, t, tw4);
+#pragma unroll
+  for (int m = 0; m < S::N1; ++m) {
+    *reinterpret_cast<float4*>(tile + (t + S::T * m) * kTile) = make_float4(v[m].re.x, v[m].im.x, v[m].re.y, v[m].im.y);
   }
 }
 
@@ -504,6 +557,8 @@ int coded_check(int n, int ds, const void* a, const void* b, const void* t2, con
     if (!st) st = ensure_smem((const void*)coded_cols<1, false, N>, cs);
     if (!st) st = ensure_smem((const void*)coded_cols<3, false, N>, cs);
     if (!st) st = ensure_smem((const void*)coded_cols<3, true, N>, cs);
+    if (!st) st = ensure_smem((const void*)coded_cols_filter_pair<false, N>, ColPairCfg<N>::kExchBytes + ColPairCfg<N>::kTwBytes);
+    if (!st) st = ensure_smem((const void*)coded_cols_filter_pair<true, N>, ColPairCfg<N>::kExchBytes + ColPairCfg<N>::kTwBytes);
     if (!st) st = ensure_smem((const void*)coded_cols<7, false, N>, cs);
     if (!st) st = ensure_smem((const void*)coded_rows_mask<N>, CodedRowCfg<N>::smem(lines128, 1));
     if (!st) st = ensure_smem((const void*)coded_rows_pool<kCodedSweep, N>, pool);
@@ -537,6 +592,16 @@ void launch_cols(const CodedGeom& g, int nf, const float2* t1, const float2* t2,
   prof_begin(kCodedCols, s);
   dispatch_pow2(g.n, [&](auto NT) {
     constexpr int N = decltype(NT)::value;
+    if constexpr (STAGE == 3) {
+      // the paired kernel reads T2 two columns at a time (16-byte loads)
+      if ((reinterpret_cast<uintptr_t>(t2) & 15) == 0) {
+        using C = ColPairCfg<N>;
+        dim3 grid(num_tiles(N), nf);
+        coded_cols_filter_pair<CONJ, N><<<grid, C::kThreads, C::kExchBytes + C::kTwBytes, s>>>(g.frames, t2, inv_n,
+                                                                                             g.plan.tw);
+        return;
+      }
+    }
     dim3 grid(num_tiles(N) * (kTile / kColsPerCta), nf);
     coded_cols<STAGE, CONJ, N><<<grid, ColPass<N>::kThreads, kColsPerCta * ColPass<N>::LP * (int)sizeof(float2), s>>>(
         g.frames, g.ospec, t1, t2, shifts, inv_n, g.gospec, g.plan.tw);
