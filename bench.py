@@ -209,21 +209,23 @@ class Fourier(Conventional):
 class Coded(Conventional):
     """Coded / near-field ptychography (config 3): 1024^2 field, 64 shifts, ds 4."""
 
-    def __init__(self, name, n, count, ds, photons, nearfield):
+    def __init__(self, name, n, count, ds, photons, nearfield, loss="mse"):
         self.name, self.n_obj, self.batch, self.ds, self.photons = name, n, count, ds, photons
         self.nearfield = nearfield
+        self.loss = loss  # "mse" or train_coded.py's fd_loss ("fd-isotropic" / "fd-anisotropic")
         self.p = n
 
     def metric(self):
         kind = "near-field" if self.nearfield else "coded"
-        return f"fwd+adj sweeps/s ({kind} {self.batch}×{self.n_obj}², ds {self.ds})"
+        tail = "" if self.loss == "mse" else f", {self.loss} loss"
+        return f"fwd+adj sweeps/s ({kind} {self.batch}×{self.n_obj}², ds {self.ds}{tail})"
 
     def bytes_per_sweep(self):
         n2 = float(self.n_obj) ** 2
         return 240.125 * n2 * self.batch + 64.0 * n2
 
     def config(self):
-        return {"workload": self.name, "modality": "near-field" if self.nearfield else "coded",
+        return {"workload": self.name, "modality": "near-field" if self.nearfield else "coded", "loss": self.loss,
                 "positions": self.batch, "field": [self.n_obj, self.n_obj], "downsample": self.ds,
                 "pixel_um": 1.85, "wavelength_um": 0.5, "z_mm": 2.0,
                 "z1_um": None if self.nearfield else 396.95, "mask": "binary 50% fill",
@@ -263,26 +265,30 @@ class Coded(Conventional):
         from ptychox_b200 import _abi
         from ptychox_b200._utils import workspace
 
+        if self.loss != "mse":
+            return workspace(_abi.query("ptx_coded_fd_workspace_bytes", self.n_obj, self.batch, self.ds), dev)
         return workspace(_abi.query("ptx_coded_workspace_bytes", self.n_obj, self.batch), dev)
 
     def sweep(self, prob, ws):
         from ptychox_b200.coded import coded_sweep
 
         return coded_sweep(prob["obj"], prob["aux"], prob["t1"], prob["t2"], prob["pos"], self.ds, prob["meas"],
-                           prob["scale"], ws=ws)
+                           prob["scale"], ws=ws, loss=self.loss)
 
     def loss_api(self, obj, aux, pos, prob):
         from ptychox_b200 import ptychoX_coded_loss, ptychoX_nearfield_loss
 
         if self.nearfield:
-            return ptychoX_nearfield_loss(obj, aux, prob["t2"], pos, self.ds, prob["meas"], prob["scale"])
-        return ptychoX_coded_loss(obj, aux, prob["t1"], prob["t2"], pos, self.ds, prob["meas"], prob["scale"])
+            return ptychoX_nearfield_loss(obj, aux, prob["t2"], pos, self.ds, prob["meas"], prob["scale"],
+                                          loss=self.loss)
+        return ptychoX_coded_loss(obj, aux, prob["t1"], prob["t2"], pos, self.ds, prob["meas"], prob["scale"],
+                                  loss=self.loss)
 
     def cpu_sweep(self, h, meas, scale, k, workers):
         from oracle import ptycho_oracle as O
 
         O.coded_sweep(h["obj"], h["aux"], h["t1"], h["t2"], h["pos"][:k], self.ds, meas[:k], scale, fp64=False,
-                      workers=workers)
+                      workers=workers, loss=self.loss)
 
 
 WORKLOADS = {
@@ -293,6 +299,7 @@ WORKLOADS = {
         Fourier("fourier-225x256-1024", 1024, 256, 15, 5e3),
         Coded("coded-64x1024-ds4", 1024, 64, 4, 2e3, nearfield=False),
         Coded("nearfield-64x1024-ds4", 1024, 64, 4, 2e3, nearfield=True),
+        Coded("coded-fd-64x1024-ds4", 1024, 64, 4, 2e3, nearfield=False, loss="fd-isotropic"),
     ]
 }
 DEFAULT_WORKLOAD = "conventional-900x512-2048"

@@ -202,6 +202,22 @@ int ptx_coded_sweep(const float* object, const float* coded_surface,
                     double* loss, float* grad_object, float* grad_coded,
                     void* workspace, size_t workspace_bytes, void* stream);
 
+/* Sweep with the periodic finite-difference data loss of python/train_coded.py:101-107
+ * (`fd_loss`, the `--loss fd-isotropic` / `fd-anisotropic` options of train_coded.py:237)
+ * in place of the MSE: D = A - sqrt(scale * I), dx / dy the periodic forward differences
+ * of D along x / y, loss = sum sqrt(dx^2 + dy^2 + 1e-5) (isotropic != 0) or
+ * sum |dx| + |dy|, summed (not averaged) in FP64; gradients OVERWRITTEN.  The loss couples
+ * neighbouring pixels, so the pooled amplitudes are materialised: the sweep runs the
+ * forward passes (keeping x and the sensor fields), a stencil pass for dL/dA, and the
+ * adjoint passes, all inside the workspace (ptx_coded_fd_workspace_bytes). */
+size_t ptx_coded_fd_workspace_bytes(int n, int batch, int downsample);
+int ptx_coded_sweep_fd(const float* object, const float* coded_surface,
+                       const float* transfer_1, const float* transfer_2, int n,
+                       const float* shifts_xy, int batch, int downsample,
+                       const uint16_t* measured, float scale, int isotropic,
+                       double* loss, float* grad_object, float* grad_coded,
+                       void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---- optimiser step -------------------------------------------------------------
  * Adam on a complex64 parameter with torch.optim.Adam semantics (the reference drivers'
  * optimiser, python/train_ptychography.py:500-507): the (re, im) pairs are independent

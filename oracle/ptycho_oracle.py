@@ -47,6 +47,7 @@ import scipy.fft as _sfft
 __all__ = [
     "measured_amplitude",
     "mse_loss_and_grad",
+    "fd_loss_and_grad",
     "base_forward",
     "base_backward",
     "base_sweep",
@@ -123,6 +124,31 @@ def mse_loss_and_grad(pred: np.ndarray, observed: np.ndarray, fp64: bool = True)
     numel = diff.size
     loss = float(np.sum(diff.astype(np.float64) ** 2) / numel)
     grad = (2.0 / numel) * diff
+    return loss, grad.astype(rd)
+
+
+def fd_loss_and_grad(pred: np.ndarray, observed: np.ndarray, isotropic: bool = True, fp64: bool = True):
+    """The periodic finite-difference data loss of ``train_coded.py:101-107`` and its gradient.
+
+    ``D = pred - observed``; ``dx = roll(D, -1, -1) - D``, ``dy = roll(D, -1, -2) - D`` (periodic
+    in the last two axes); loss ``sum(sqrt(dx^2 + dy^2 + 1e-5))`` (isotropic) or
+    ``sum(|dx| + |dy|)``, summed, not averaged.  Gradient w.r.t. ``pred``: every pixel enters
+    its own term and those of its left and upper neighbours,
+    ``g = -(ux + uy) + roll(ux, 1, -1) + roll(uy, 1, -2)`` with ``(ux, uy) = (dx, dy) / m``
+    (isotropic, ``m`` the square root) or ``(sign dx, sign dy)``.
+    """
+    rd = np.float64 if fp64 else np.result_type(pred.dtype, np.float32).type
+    d = pred.astype(rd) - observed.astype(rd)
+    dx = np.roll(d, -1, axis=-1) - d
+    dy = np.roll(d, -1, axis=-2) - d
+    if isotropic:
+        m = np.sqrt(dx * dx + dy * dy + rd(1e-5))
+        loss = float(np.sum(m.astype(np.float64)))
+        ux, uy = dx / m, dy / m
+    else:
+        loss = float(np.sum(np.abs(dx).astype(np.float64) + np.abs(dy).astype(np.float64)))
+        ux, uy = np.sign(dx), np.sign(dy)
+    grad = -(ux + uy) + np.roll(ux, 1, axis=-1) + np.roll(uy, 1, axis=-2)
     return loss, grad.astype(rd)
 
 
@@ -336,22 +362,30 @@ def coded_backward(grad_output, x_forward, sensor_field, amplitude, coded_surfac
 
 
 def coded_sweep(object_field, coded_surface, transfer_1, transfer_2, shifts_xy, downsample,
-                measured_u16, scale, fp64: bool = True, workers: int | None = None):
-    """Forward, amplitude-MSE loss, adjoint for coded ptychography (``train_coded.py:225-237``)."""
+                measured_u16, scale, fp64: bool = True, workers: int | None = None, loss: str = "mse"):
+    """Forward, data loss, adjoint for coded ptychography (``train_coded.py:225-237``).
+
+    ``loss``: ``"mse"`` (``F.mse_loss``), ``"fd-isotropic"`` or ``"fd-anisotropic"``
+    (``fd_loss``, ``train_coded.py:101-107``)."""
     _, xf, sensor, amp = coded_forward(object_field, coded_surface, transfer_1, transfer_2,
                                        shifts_xy, downsample, fp64, workers)
     observed = measured_amplitude(measured_u16, scale)
-    loss, g = mse_loss_and_grad(amp, observed, fp64=fp64)
+    if loss == "mse":
+        loss, g = mse_loss_and_grad(amp, observed, fp64=fp64)
+    elif loss in ("fd-isotropic", "fd-anisotropic"):
+        loss, g = fd_loss_and_grad(amp, observed, isotropic=loss == "fd-isotropic", fp64=fp64)
+    else:
+        raise ValueError(f"unknown loss {loss!r}")
     go, gm = coded_backward(g, xf, sensor, amp, coded_surface, transfer_1, transfer_2, shifts_xy,
                             downsample, workers)
     return loss, go, gm
 
 
 def nearfield_sweep(object_field, probe_field, transfer, shifts_xy, downsample, measured_u16, scale,
-                    fp64: bool = True, workers: int | None = None):
+                    fp64: bool = True, workers: int | None = None, loss: str = "mse"):
     """Near-field = coded with ``transfer_1 = 1`` (``adPtychoX_nearf.m:44-62``)."""
     return coded_sweep(object_field, probe_field, None, transfer, shifts_xy, downsample,
-                       measured_u16, scale, fp64, workers)
+                       measured_u16, scale, fp64, workers, loss)
 
 
 # ----------------------------------------------------------------------------------------

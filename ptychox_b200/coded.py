@@ -162,51 +162,70 @@ def ptychoX_nearfield(object_field, probe_field, transfer, shifts_xy, downsample
 nearfield_ptychography = ptychoX_nearfield
 
 
-def coded_sweep(obj, mask, t1, t2, shifts, downsample, measured, scale, ws=None):
-    """One fused coded (or near-field, ``t1=None``) sweep; returns ``(loss, grad_object, grad_mask)``."""
+LOSSES = ("mse", "fd-isotropic", "fd-anisotropic")
+
+
+def coded_sweep(obj, mask, t1, t2, shifts, downsample, measured, scale, ws=None, loss="mse"):
+    """One fused coded (or near-field, ``t1=None``) sweep; returns ``(loss, grad_object, grad_mask)``.
+
+    ``loss``: ``"mse"`` (``F.mse_loss``) or the periodic finite-difference loss of
+    ``train_coded.py:101-107`` (``"fd-isotropic"`` / ``"fd-anisotropic"``).
+    """
+    if loss not in LOSSES:
+        raise ValueError(f"loss must be one of {LOSSES}, got {loss!r}")
     dev = obj.device
     n, batch = obj.shape[0], shifts.shape[0]
-    loss = torch.empty((), dtype=torch.float64, device=dev)
+    out = torch.empty((), dtype=torch.float64, device=dev)
     go = torch.empty_like(obj)
     gm = torch.empty_like(mask)
-    if ws is None:
-        ws, _ = _ws(n, batch, dev)
     with torch.cuda.device(dev):
-        _abi.call("ptx_coded_sweep", ptr(obj), ptr(mask), ptr(t1), ptr(t2), n, ptr(shifts), batch, int(downsample),
-                  ptr(measured), float(scale), ptr(loss), ptr(go), ptr(gm), ptr(ws), ws.numel(), stream_handle(dev))
-    return loss, go, gm
+        if loss == "mse":
+            if ws is None:
+                ws, _ = _ws(n, batch, dev)
+            _abi.call("ptx_coded_sweep", ptr(obj), ptr(mask), ptr(t1), ptr(t2), n, ptr(shifts), batch,
+                      int(downsample), ptr(measured), float(scale), ptr(out), ptr(go), ptr(gm), ptr(ws), ws.numel(),
+                      stream_handle(dev))
+        else:
+            if ws is None:
+                ws = workspace(_abi.query("ptx_coded_fd_workspace_bytes", n, batch, int(downsample)), dev)
+            _abi.call("ptx_coded_sweep_fd", ptr(obj), ptr(mask), ptr(t1), ptr(t2), n, ptr(shifts), batch,
+                      int(downsample), ptr(measured), float(scale), int(loss == "fd-isotropic"), ptr(out), ptr(go),
+                      ptr(gm), ptr(ws), ws.numel(), stream_handle(dev))
+    return out, go, gm
 
 
 class PtychoXCodedLossFunction(torch.autograd.Function):
     @staticmethod
     def forward(ctx, object_field, coded_surface, transfer_1, transfer_2, shifts_xy, downsample, measured,  # type: ignore[override]
-                scale):
+                scale, loss="mse"):
         obj, mask, t1, t2, shifts = _prepare(object_field, coded_surface, transfer_1, transfer_2, shifts_xy,
                                              downsample)
         n, ds = obj.shape[0], int(downsample)
         meas = as_u16(measured, obj.device)
         if tuple(meas.shape) != (shifts.shape[0], n // ds, n // ds):
             raise ValueError("measured must have shape [batch, H/downsample, W/downsample].")
-        loss, go, gm = coded_sweep(obj, mask, t1, t2, shifts, ds, meas, scale)
+        value, go, gm = coded_sweep(obj, mask, t1, t2, shifts, ds, meas, scale, loss=loss)
         ctx.save_for_backward(go, gm)
-        return loss
+        return value
 
     @staticmethod
     def backward(ctx, grad_loss):  # type: ignore[override]
         go, gm = ctx.saved_tensors
         g = grad_loss.to(torch.float32)
-        return go * g, gm * g, None, None, None, None, None, None
+        return go * g, gm * g, None, None, None, None, None, None, None
 
 
 def ptychoX_coded_loss(object_field, coded_surface, transfer_1, transfer_2, shifts_xy, downsample, measured,
-                       scale) -> torch.Tensor:
-    """Fused ``F.mse_loss(ptychoX_coded(...), sqrt(scale * measured))`` as an FP64 scalar."""
+                       scale, loss: str = "mse") -> torch.Tensor:
+    """Fused ``F.mse_loss(ptychoX_coded(...), sqrt(scale * measured))`` as an FP64 scalar;
+    ``loss="fd-isotropic"`` / ``"fd-anisotropic"`` gives ``fd_loss`` (``train_coded.py:101-107``)."""
     return PtychoXCodedLossFunction.apply(object_field, coded_surface, transfer_1, transfer_2, shifts_xy, downsample,
-                                          measured, scale)
+                                          measured, scale, loss)
 
 
 def ptychoX_nearfield_loss(object_field, probe_field, transfer, shifts_xy, downsample, measured,
-                           scale) -> torch.Tensor:
-    """Fused near-field sweep (``transfer_1 = 1``) as an FP64 scalar."""
+                           scale, loss: str = "mse") -> torch.Tensor:
+    """Fused near-field sweep (``transfer_1 = 1``) as an FP64 scalar; ``loss`` as in
+    ``ptychoX_coded_loss``."""
     return PtychoXCodedLossFunction.apply(object_field, probe_field, None, transfer, shifts_xy, downsample, measured,
-                                          scale)
+                                          scale, loss)

@@ -485,6 +485,61 @@ __global__ void __launch_bounds__(128, 2) coded_rows_grad_mask(
   }
 }
 
+// ---- finite-difference data loss ---------------------------------------------------------
+// fd_loss of train_coded.py:101-107 on the pooled amplitudes A [batch, h, w] against the
+// decoded counts Y = sqrt(I scale): D = A - Y, dx = D(y, x+1) - D, dy = D(y+1, x) - D
+// (periodic), loss = sum sqrt(dx^2 + dy^2 + 1e-5) (isotropic) or sum |dx| + |dy|, and
+// dL/dA = -(ux + uy)(y, x) + ux(y, x-1) + uy(y-1, x) with (ux, uy) = (dx, dy) / m or the
+// signs.  One thread per pixel; the 7-point neighbourhood of D is re-derived from A and I.
+__device__ __forceinline__ float fd_diff(const float* __restrict__ amp, const uint16_t* __restrict__ meas,
+                                         size_t base, int h, int w, int y, int x, float scale) {
+  y = y < 0 ? y + h : (y >= h ? y - h : y);
+  x = x < 0 ? x + w : (x >= w ? x - w : x);
+  const size_t i = base + (size_t)y * w + x;
+  return amp[i] - sqrtf(static_cast<float>(meas[i]) * scale);
+}
+
+__device__ __forceinline__ void fd_unit(float dx, float dy, bool isotropic, float& ux, float& uy, float& m) {
+  if (isotropic) {
+    m = sqrtf(fmaf(dx, dx, fmaf(dy, dy, 1e-5f)));
+    ux = dx / m;
+    uy = dy / m;
+  } else {
+    m = fabsf(dx) + fabsf(dy);
+    ux = dx > 0.f ? 1.f : (dx < 0.f ? -1.f : 0.f);
+    uy = dy > 0.f ? 1.f : (dy < 0.f ? -1.f : 0.f);
+  }
+}
+
+__global__ void __launch_bounds__(256) fd_loss_kernel(const float* __restrict__ amp, const uint16_t* __restrict__ meas,
+                                                      float scale, long long total, int h, int w, int isotropic,
+                                                      float* __restrict__ grad_amp, double* __restrict__ loss) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double part = 0.0;
+  if (i < total) {
+    const long long hw = (long long)h * w;
+    const long long b = i / hw;
+    const int y = static_cast<int>((i - b * hw) / w);
+    const int x = static_cast<int>(i - b * hw - (long long)y * w);
+    const size_t base = (size_t)(b * hw);
+    const bool iso = isotropic != 0;
+    const float d = fd_diff(amp, meas, base, h, w, y, x, scale);
+    const float dr = fd_diff(amp, meas, base, h, w, y, x + 1, scale);
+    const float dd = fd_diff(amp, meas, base, h, w, y + 1, x, scale);
+    const float dl = fd_diff(amp, meas, base, h, w, y, x - 1, scale);
+    const float ddl = fd_diff(amp, meas, base, h, w, y + 1, x - 1, scale);
+    const float du = fd_diff(amp, meas, base, h, w, y - 1, x, scale);
+    const float dur = fd_diff(amp, meas, base, h, w, y - 1, x + 1, scale);
+    float ux, uy, m, uxl, uyl, ml, uxu, uyu, mu;
+    fd_unit(dr - d, dd - d, iso, ux, uy, m);           // this pixel's term
+    fd_unit(d - dl, ddl - dl, iso, uxl, uyl, ml);      // left neighbour's term
+    fd_unit(dur - du, d - du, iso, uxu, uyu, mu);      // upper neighbour's term
+    grad_amp[i] = -(ux + uy) + uxl + uyu;
+    part = static_cast<double>(m);
+  }
+  block_add_double(part, 1.0, loss);
+}
+
 // ---------------------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------------------
@@ -774,6 +829,66 @@ int ptx_coded_sweep(const float* object, const float* coded_surface, const float
   }
   launch_fft2<true>(g.gospec, n, reinterpret_cast<float2*>(grad_object), g.tmp, g.plan, s);
   return cuda_status(cudaGetLastError(), "ptx_coded_sweep launch");
+}
+
+
+size_t ptx_coded_fd_workspace_bytes(int n, int batch, int downsample) {
+  if (n <= 0 || batch < 0 || downsample <= 0) return 0;
+  const size_t b = (size_t)std::max(batch, 1);
+  const size_t field = (size_t)n * n * sizeof(float2);
+  const size_t pooled = (size_t)(n / downsample) * (n / downsample) * sizeof(float);
+  auto up = [](size_t x) { return (x + 255) / 256 * 256; };
+  return 2 * up(b * field) + 2 * up(b * pooled) + ptx_coded_workspace_bytes(n, batch);
+}
+
+int ptx_coded_sweep_fd(const float* object, const float* coded_surface, const float* transfer_1,
+                       const float* transfer_2, int n, const float* shifts_xy, int batch, int downsample,
+                       const uint16_t* measured, float scale, int isotropic, double* loss, float* grad_object,
+                       float* grad_coded, void* workspace, size_t workspace_bytes, void* stream) {
+  if (!loss || !grad_object || !grad_coded || !workspace || (!measured && batch > 0)) {
+    return set_error(PTX_ERR_INVALID_ARGUMENT, "null pointer argument");
+  }
+  if (n <= 0 || downsample <= 0 || batch < 0) return set_error(PTX_ERR_INVALID_ARGUMENT, "non-positive shape");
+  if (!(scale > 0.f)) return set_error(PTX_ERR_INVALID_ARGUMENT, "scale must be positive");
+  if (reinterpret_cast<uintptr_t>(workspace) & 255) {
+    return set_error(PTX_ERR_INVALID_ARGUMENT, "workspace must start on a 256-byte boundary");
+  }
+  const size_t need = ptx_coded_fd_workspace_bytes(n, batch, downsample);
+  if (workspace_bytes < need) {
+    return set_error(PTX_ERR_WORKSPACE, "workspace of %zu bytes is smaller than the %zu bytes needed",
+                     workspace_bytes, need);
+  }
+  // workspace: x fields | sensor fields | pooled amplitudes | dL/dA | forward/backward frames
+  auto up = [](size_t x) { return (x + 255) / 256 * 256; };
+  const size_t b = (size_t)std::max(batch, 1);
+  const size_t field = (size_t)n * n * sizeof(float2);
+  const int h = n / downsample;
+  const size_t pooled = (size_t)h * h * sizeof(float);
+  char* p = static_cast<char*>(workspace);
+  float* xf = reinterpret_cast<float*>(p);
+  p += up(b * field);
+  float* sensor = reinterpret_cast<float*>(p);
+  p += up(b * field);
+  float* amp = reinterpret_cast<float*>(p);
+  p += up(b * pooled);
+  float* gamp = reinterpret_cast<float*>(p);
+  p += up(b * pooled);
+  const size_t inner = workspace_bytes - static_cast<size_t>(p - static_cast<char*>(workspace));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (int st = ptx_coded_forward(object, coded_surface, transfer_1, transfer_2, n, shifts_xy, batch, downsample, xf,
+                                 sensor, amp, p, inner, stream)) {
+    return st;
+  }
+  cudaMemsetAsync(loss, 0, sizeof(double), s);
+  const long long total = (long long)batch * h * h;
+  if (total > 0) {
+    prof_begin(kMiscKernel, s);
+    fd_loss_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, s>>>(amp, measured, scale, total, h, h,
+                                                                            isotropic, gamp, loss);
+    prof_end(kMiscKernel, s);
+  }
+  return ptx_coded_backward(gamp, xf, sensor, amp, coded_surface, transfer_1, transfer_2, n, shifts_xy, batch,
+                            downsample, grad_object, grad_coded, p, inner, stream);
 }
 
 }  // extern "C"

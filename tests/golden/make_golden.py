@@ -12,7 +12,10 @@ It imports ``ptychoX`` from that directory and writes ``tests/golden/*.npz``:
 * ``sweep_*_fp64.npz`` — small config-shaped problems run through the reference operator
   in complex128 followed by ``F.mse_loss(pred, observed)`` and ``.backward()`` (the
   training drivers' step, ``train_ptychography.py:549-557``), with uint16 Poisson counts
-  decoded as ``sqrt(float32(I) * float32(scale))``: loss and gradients.
+  decoded as ``sqrt(float32(I) * float32(scale))``: loss and gradients;
+* ``sweep_coded_fd_{iso,aniso}_fp64.npz`` — the coded problem with the reference's own
+  ``fd_loss`` (``train_coded.py:101-107``, imported from the reference's ``train_coded``
+  module) in place of the MSE.
 
 The fixtures are small (a few hundred KB in total) and are the parity pin of the
 numpy oracle (``oracle/``) and of the CUDA library.
@@ -83,10 +86,10 @@ def _observed(counts: np.ndarray, scale: float) -> torch.Tensor:
     return torch.from_numpy(amp32.astype(np.float64))
 
 
-def _loss_step(fn, params, observed):
+def _loss_step(fn, params, observed, loss_fn=None):
     leaves = [torch.from_numpy(p.astype(np.complex128)).requires_grad_(True) for p in params]
     pred = fn(*leaves)
-    loss = F.mse_loss(pred, observed)
+    loss = F.mse_loss(pred, observed) if loss_fn is None else loss_fn(pred, observed)
     loss.backward()
     return float(loss.item()), [_np(x.grad) for x in leaves]
 
@@ -131,7 +134,7 @@ def sweep_fpm(ptychoX, name, n, h, leds_grid, photons, seed):
              grad_object=g_obj, grad_pupil=g_pup)
 
 
-def sweep_coded(ptychoX, name, n, ds, count, photons, seed, nearfield):
+def sweep_coded(ptychoX, name, n, ds, count, photons, seed, nearfield, loss_fn=None):
     rng = np.random.default_rng(seed)
     obj_true = synth.random_object(n, n, rng)
     mask = synth.binary_mask(n, 0.5, rng)
@@ -149,10 +152,18 @@ def sweep_coded(ptychoX, name, n, ds, count, photons, seed, nearfield):
     obj = (obj_true * (1.0 + 0.15 * rng.standard_normal(obj_true.shape))).astype(np.complex64)
     msk = (mask * (1.0 + 0.1 * rng.standard_normal(mask.shape)) + 0.05).astype(np.complex64)
     loss, (g_obj, g_mask) = _loss_step(lambda o, m: ptychoX.ptychoX_coded(o, m, t1_t, t2_t, sh_t, ds), [obj, msk],
-                                       _observed(counts, scale))
+                                       _observed(counts, scale), loss_fn)
     np.savez(HERE / name, object=obj, mask=msk, transfer_1=t1, transfer_2=t2, shifts=shifts, downsample=ds,
              measured=counts, scale=np.float32(scale), loss=loss, grad_object=g_obj, grad_mask=g_mask,
              nearfield=nearfield)
+
+
+def fd_cases(ptychoX):
+    import train_coded  # the reference's coded training driver (defines fd_loss)
+
+    for iso, tag in ((True, "iso"), (False, "aniso")):
+        sweep_coded(ptychoX, f"sweep_coded_fd_{tag}_fp64.npz", 32, 2, 4, 200.0, seed=16, nearfield=False,
+                    loss_fn=lambda p, o, iso=iso: train_coded.fd_loss(p, o, isotropic=iso))
 
 
 def main(ref_python_dir: str) -> None:
@@ -166,8 +177,16 @@ def main(ref_python_dir: str) -> None:
     sweep_fpm(ptychoX, "sweep_fpm_fp64.npz", 64, 16, 3, 500.0, seed=13)
     sweep_coded(ptychoX, "sweep_coded_fp64.npz", 32, 2, 4, 200.0, seed=14, nearfield=False)
     sweep_coded(ptychoX, "sweep_nearfield_fp64.npz", 32, 4, 3, 200.0, seed=15, nearfield=True)
+    fd_cases(ptychoX)
     print("wrote", sorted(p.name for p in HERE.glob("*.npz")))
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/python")
+    if len(sys.argv) > 2 and sys.argv[2] == "fd":  # only the fd_loss fixtures
+        sys.dont_write_bytecode = True
+        sys.path.insert(0, sys.argv[1])
+        import ptychoX  # noqa: E402
+
+        fd_cases(ptychoX)
+    else:
+        main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/python")

@@ -19,11 +19,11 @@ def cuda(a):
     return torch.from_numpy(np.ascontiguousarray(a)).cuda()
 
 
-def run_sweep(obj, mask, t1, t2, shifts, ds, meas, scale):
+def run_sweep(obj, mask, t1, t2, shifts, ds, meas, scale, loss="mse"):
     from ptychox_b200.coded import coded_sweep
 
     loss, go, gm = coded_sweep(cuda(obj), cuda(mask), None if t1 is None else cuda(t1), cuda(t2),
-                               cuda(shifts.astype(np.float32)), ds, cuda(meas), scale)
+                               cuda(shifts.astype(np.float32)), ds, cuda(meas), scale, loss=loss)
     torch.cuda.synchronize()
     return float(loss.item()), go.cpu().numpy(), gm.cpu().numpy()
 
@@ -129,3 +129,47 @@ def test_input_errors():
     w = torch.zeros(96, 96, dtype=torch.complex64, device="cuda")
     with pytest.raises(ValueError):
         ptychoX_coded(w, w, w, w, sh, 2)  # 96 is not a power of two
+
+
+@pytest.mark.parametrize("name,loss", [("sweep_coded_fd_iso_fp64.npz", "fd-isotropic"),
+                                       ("sweep_coded_fd_aniso_fp64.npz", "fd-anisotropic")])
+def test_fd_loss_golden(name, loss):
+    """fd_loss (train_coded.py:101-107) through ptx_coded_sweep_fd against the reference's
+    own loss and gradients.  Bar: 1e-5, or twice the error of the reference's FP32
+    formulation where FP32 itself limits the result (the loss differences amplify the FP32
+    error of the pooled amplitudes)."""
+    g = load_golden(name)
+    args = (g["object"], g["mask"], g["transfer_1"], g["transfer_2"], g["shifts"], int(g["downsample"]),
+            g["measured"], float(g["scale"]))
+    loss_v, go, gm = run_sweep(*args, loss=loss)
+    ref_loss, ref_go, ref_gm = O.coded_sweep(*args, fp64=False, loss=loss)
+    assert abs(loss_v - float(g["loss"])) <= fp32_tol(abs(ref_loss - float(g["loss"])) / abs(float(g["loss"]))) * abs(
+        float(g["loss"]))
+    assert rel_l2(go, g["grad_object"]) < fp32_tol(rel_l2(ref_go, g["grad_object"]))
+    assert rel_l2(gm, g["grad_mask"]) < fp32_tol(rel_l2(ref_gm, g["grad_mask"]))
+
+
+@pytest.mark.parametrize("nearfield,loss", [(False, "fd-isotropic"), (True, "fd-anisotropic")])
+def test_fd_loss_vs_oracle_and_autograd(nearfield, loss):
+    """A 128^2 field, 6 shifts, ds 2: the fd-loss sweep against the FP64 oracle, and the
+    autograd entry point (ptychoX_coded_loss / ptychoX_nearfield_loss) against the sweep."""
+    from ptychox_b200 import ptychoX_coded_loss, ptychoX_nearfield_loss
+
+    obj, mask, t1, t2, shifts, meas, scale = coded_problem(128, 6, 8.0, 2, 500.0, seed=21, nearfield=nearfield)
+    loss_v, go, gm = run_sweep(obj, mask, t1, t2, shifts, 2, meas, scale, loss=loss)
+    ref = O.coded_sweep(obj, mask, t1, t2, shifts, 2, meas, scale, loss=loss)
+    ref32 = O.coded_sweep(obj, mask, t1, t2, shifts, 2, meas, scale, fp64=False, loss=loss)
+    assert abs(loss_v - ref[0]) <= fp32_tol(abs(ref32[0] - ref[0]) / abs(ref[0])) * abs(ref[0])
+    assert rel_l2(go, ref[1]) < fp32_tol(rel_l2(ref32[1], ref[1]))
+    assert rel_l2(gm, ref[2]) < fp32_tol(rel_l2(ref32[2], ref[2]))
+    o = cuda(obj).requires_grad_(True)
+    m = cuda(mask).requires_grad_(True)
+    sh = cuda(shifts.astype(np.float32))
+    if nearfield:
+        val = ptychoX_nearfield_loss(o, m, cuda(t2), sh, 2, cuda(meas), scale, loss=loss)
+    else:
+        val = ptychoX_coded_loss(o, m, cuda(t1), cuda(t2), sh, 2, cuda(meas), scale, loss=loss)
+    val.backward()
+    assert abs(float(val.item()) - loss_v) <= 1e-12 * abs(loss_v)
+    assert rel_l2(o.grad.cpu().numpy(), go) < 1e-6 and rel_l2(m.grad.cpu().numpy(), gm) < 1e-6
+

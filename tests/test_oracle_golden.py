@@ -82,3 +82,15 @@ def test_nearfield_is_coded_with_unit_transfer():
                           g["measured"], float(g["scale"]))
     assert abs(a[0] - b[0]) <= 1e-13 * abs(a[0])
     assert rel_l2(a[1], b[1]) < 1e-13 and rel_l2(a[2], b[2]) < 1e-13
+
+
+@pytest.mark.parametrize("name,loss", [("sweep_coded_fd_iso_fp64.npz", "fd-isotropic"),
+                                       ("sweep_coded_fd_aniso_fp64.npz", "fd-anisotropic")])
+def test_sweep_coded_fd_loss(name, loss):
+    """The fd_loss data term (train_coded.py:101-107) against the reference's own function."""
+    g = load_golden(name)
+    got, go, gm = O.coded_sweep(g["object"], g["mask"], g["transfer_1"], g["transfer_2"], g["shifts"],
+                                int(g["downsample"]), g["measured"], float(g["scale"]), loss=loss)
+    assert abs(got - float(g["loss"])) <= TOL_F64 * abs(float(g["loss"]))
+    assert rel_l2(go, g["grad_object"]) < TOL_F64
+    assert rel_l2(gm, g["grad_mask"]) < TOL_F64
