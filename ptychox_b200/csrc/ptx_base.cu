@@ -891,15 +891,14 @@ int ptx_base_sweep(const float* sample, int sample_h, int sample_w, const float*
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   float2* GS = reinterpret_cast<float2*>(grad_sample);
   float2* GP = reinterpret_cast<float2*>(grad_probe);
-  cudaMemsetAsync(GS, 0, sizeof(float2) * (size_t)sample_h * sample_w, s);
-  cudaMemsetAsync(GP, 0, sizeof(float2) * (size_t)probe_h * probe_w, s);
-  cudaMemsetAsync(loss, 0, sizeof(double), s);
-  cudaMemsetAsync(g.err, 0, sizeof(unsigned), s);
   const double numel = (double)batch * probe_h * probe_w;
   const float grad_scale = static_cast<float>(2.0 / std::max(numel, 1.0));
-  prof_begin(kMiscKernel, s);
-  decode_lut_kernel<<<kLutEntries / 256, 256, 0, s>>>(g.lut, scale);
-  prof_end(kMiscKernel, s);
+  {
+    const size_t ns = (size_t)sample_h * sample_w, np = (size_t)probe_h * probe_w;
+    prof_begin(kMiscKernel, s);
+    sweep_prologue_kernel<<<prologue_blocks(ns, sm_count()), 256, 0, s>>>(GS, ns, GP, np, loss, g.err, g.lut, scale);
+    prof_end(kMiscKernel, s);
+  }
   const float2* S = reinterpret_cast<const float2*>(sample);
   const float2* P = reinterpret_cast<const float2*>(probe);
   for (int b0 = 0; b0 < batch; b0 += g.chunk) {

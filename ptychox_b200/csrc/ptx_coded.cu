@@ -810,9 +810,13 @@ int ptx_coded_sweep(const float* object, const float* coded_surface, const float
   const float2* T1 = reinterpret_cast<const float2*>(transfer_1);
   const float2* T2 = reinterpret_cast<const float2*>(transfer_2);
   const float2* M = reinterpret_cast<const float2*>(coded_surface);
-  cudaMemsetAsync(g.gospec, 0, g.field_bytes, s);
-  cudaMemsetAsync(grad_coded, 0, g.field_bytes, s);
-  cudaMemsetAsync(loss, 0, sizeof(double), s);
+  {
+    const size_t nf = g.field_bytes / sizeof(float2);
+    prof_begin(kMiscKernel, s);
+    sweep_prologue_kernel<<<prologue_blocks(nf, sm_count()), 256, 0, s>>>(
+        g.gospec, nf, reinterpret_cast<float2*>(grad_coded), nf, loss, nullptr, nullptr, 0.f);
+    prof_end(kMiscKernel, s);
+  }
   const int lw = n / downsample;
   const double numel = (double)batch * lw * lw;
   const float grad_scale = static_cast<float>(2.0 / std::max(numel, 1.0));

@@ -559,14 +559,15 @@ int ptx_fpm_sweep(const float* object, int object_h, int object_w, const float* 
   }
   if (!(scale > 0.f)) return set_error(PTX_ERR_INVALID_ARGUMENT, "scale must be positive");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  cudaMemsetAsync(g.gspec, 0, g.spec_bytes, s);
-  cudaMemsetAsync(grad_pupil, 0, sizeof(float2) * (size_t)low_h * low_w, s);
-  cudaMemsetAsync(loss, 0, sizeof(double), s);
   const double numel = (double)batch * low_h * low_w;
   const float grad_scale = static_cast<float>(2.0 / std::max(numel, 1.0));
-  prof_begin(kMiscKernel, s);
-  decode_lut_kernel<<<kLutEntries / 256, 256, 0, s>>>(g.lut, scale);
-  prof_end(kMiscKernel, s);
+  {
+    const size_t ns = g.spec_bytes / sizeof(float2), np = (size_t)low_h * low_w;
+    prof_begin(kMiscKernel, s);
+    sweep_prologue_kernel<<<prologue_blocks(ns, sm_count()), 256, 0, s>>>(
+        g.gspec, ns, reinterpret_cast<float2*>(grad_pupil), np, loss, nullptr, g.lut, scale);
+    prof_end(kMiscKernel, s);
+  }
   launch_fft2<false>(reinterpret_cast<const float2*>(object), object_h, object_w, g.spec, 1.0f, g.tmp, g.p_ow, g.p_oh,
                      s);
   const float2* P = reinterpret_cast<const float2*>(pupil);

@@ -4,6 +4,8 @@
 #pragma once
 
 #include <cuda_runtime.h>
+
+#include <algorithm>
 #include <stdint.h>
 
 #include "ptx_pairfft.cuh"
@@ -80,6 +82,32 @@ constexpr size_t kLutBytes = kLutEntries * sizeof(float);
 static __global__ void decode_lut_kernel(float* __restrict__ lut, float scale) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c < kLutEntries) lut[c] = sqrtf(static_cast<float>(c) * scale);
+}
+
+// One launch for everything a sweep resets before its passes: zero two gradient arrays
+// (n_a and n_b complex elements), the FP64 loss and the error word, and (lut non-null)
+// build the count-decode table.  Grid-stride; any grid size works.
+static __global__ void sweep_prologue_kernel(float2* __restrict__ zero_a, size_t n_a, float2* __restrict__ zero_b,
+                                             size_t n_b, double* __restrict__ loss, unsigned* __restrict__ err,
+                                             float* __restrict__ lut, float scale) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const size_t i0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const float2 z = make_float2(0.f, 0.f);
+  for (size_t i = i0; i < n_a; i += stride) zero_a[i] = z;
+  for (size_t i = i0; i < n_b; i += stride) zero_b[i] = z;
+  if (lut) {
+    for (size_t c = i0; c < (size_t)kLutEntries; c += stride) lut[c] = sqrtf(static_cast<float>(c) * scale);
+  }
+  if (i0 == 0) {
+    if (loss) *loss = 0.0;
+    if (err) *err = 0u;
+  }
+}
+
+// Grid of sweep_prologue_kernel: about 8 elements per thread, at most 4 waves of 256-thread CTAs.
+inline unsigned prologue_blocks(size_t elements, int sms) {
+  const size_t want = (elements / 8 + 255) / 256;
+  return static_cast<unsigned>(std::max<size_t>(1, std::min<size_t>(want, (size_t)sms * 8 * 4)));
 }
 
 // 1/sqrt(s), s > 0: the rsqrtf estimate refined by one Newton-Raphson step for the
