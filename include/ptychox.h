@@ -218,6 +218,24 @@ int ptx_coded_sweep_fd(const float* object, const float* coded_surface,
                        double* loss, float* grad_object, float* grad_coded,
                        void* workspace, size_t workspace_bytes, void* stream);
 
+/* General coded / near-field sweep.  loss_kind: PTX_LOSS_MSE (as ptx_coded_sweep),
+ * PTX_LOSS_FD_ISOTROPIC / PTX_LOSS_FD_ANISOTROPIC (as ptx_coded_sweep_fd).  grad_shifts
+ * (double [batch, 2], may be NULL) receives dL/d(shifts_xy): the shifts enter only through
+ * the phase ramp R_b, so dL/d(dx_b, dy_b) = -2 pi sum_k (fx, fy) Im(conj(G_b) u_b) with
+ * u_b = fft2(O) T1 R_b and G_b its gradient -- what autograd gives through the reference's
+ * torch formulation (python/ptychoX/coded/ops.py:157-171; its CUDA operator returns no
+ * shift gradient).  Workspace: ptx_coded_sweep_ex_workspace_bytes. */
+#define PTX_LOSS_MSE 0
+#define PTX_LOSS_FD_ISOTROPIC 1
+#define PTX_LOSS_FD_ANISOTROPIC 2
+size_t ptx_coded_sweep_ex_workspace_bytes(int n, int batch, int downsample, int loss_kind);
+int ptx_coded_sweep_ex(const float* object, const float* coded_surface,
+                       const float* transfer_1, const float* transfer_2, int n,
+                       const float* shifts_xy, int batch, int downsample,
+                       const uint16_t* measured, float scale, int loss_kind,
+                       double* loss, float* grad_object, float* grad_coded, double* grad_shifts,
+                       void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---- optimiser step -------------------------------------------------------------
  * Adam on a complex64 parameter with torch.optim.Adam semantics (the reference drivers'
  * optimiser, python/train_ptychography.py:500-507): the (re, im) pairs are independent

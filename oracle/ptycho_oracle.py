@@ -330,7 +330,7 @@ def coded_forward(object_field, coded_surface, transfer_1, transfer_2, shifts_xy
 
 
 def coded_backward(grad_output, x_forward, sensor_field, amplitude, coded_surface, transfer_1,
-                   transfer_2, shifts_xy, downsample, workers: int | None = None):
+                   transfer_2, shifts_xy, downsample, workers: int | None = None, with_shifts: bool = False):
     """Adjoint of :func:`coded_forward` (what autograd computes through ``coded/ops.py:136-154``).
 
     Step order follows the reference's explicit CUDA adjoint (``coded_kernel.cu:347-424``):
@@ -358,15 +358,28 @@ def coded_backward(grad_output, x_forward, sensor_field, amplitude, coded_surfac
     conj_pre = np.conj(ramp) if transfer_1 is None else np.conj(ramp * np.asarray(transfer_1).astype(cd)[None])
     grad_spectrum = np.sum(g_big_x * conj_pre, axis=0)
     grad_object = _ifft2(grad_spectrum, workers) * n
-    return grad_object, grad_mask
+    if not with_shifts:
+        return grad_object, grad_mask
+    # Shifts (real) enter only through the ramp of u = fft2(O) T1 ramp = fft2(x_forward):
+    # du/d(dx) = 2 pi i fx u, so dL/d(dx) = Re(sum conj(G_u) du/d(dx)) = -2 pi sum fx Im(conj(G_u) u)
+    # with G_u = g_big_x the PyTorch-convention gradient of u (coded/ops.py:157-171 autograd).
+    u = _fft2(x_forward, workers)
+    z = np.imag(np.conj(g_big_x) * u).astype(np.float64)
+    fy = np.fft.fftfreq(h, d=1.0) * h
+    fx = np.fft.fftfreq(w, d=1.0) * w
+    gx = -2.0 * math.pi * np.einsum("bij,j->b", z, fx)
+    gy = -2.0 * math.pi * np.einsum("bij,i->b", z, fy)
+    return grad_object, grad_mask, np.stack([gx, gy], axis=1)
 
 
 def coded_sweep(object_field, coded_surface, transfer_1, transfer_2, shifts_xy, downsample,
-                measured_u16, scale, fp64: bool = True, workers: int | None = None, loss: str = "mse"):
+                measured_u16, scale, fp64: bool = True, workers: int | None = None, loss: str = "mse",
+                with_shifts: bool = False):
     """Forward, data loss, adjoint for coded ptychography (``train_coded.py:225-237``).
 
     ``loss``: ``"mse"`` (``F.mse_loss``), ``"fd-isotropic"`` or ``"fd-anisotropic"``
-    (``fd_loss``, ``train_coded.py:101-107``)."""
+    (``fd_loss``, ``train_coded.py:101-107``).  ``with_shifts``: also return the gradient
+    w.r.t. ``shifts_xy`` ([batch, 2], what autograd gives through ``coded/ops.py:157-171``)."""
     _, xf, sensor, amp = coded_forward(object_field, coded_surface, transfer_1, transfer_2,
                                        shifts_xy, downsample, fp64, workers)
     observed = measured_amplitude(measured_u16, scale)
@@ -376,9 +389,9 @@ def coded_sweep(object_field, coded_surface, transfer_1, transfer_2, shifts_xy, 
         loss, g = fd_loss_and_grad(amp, observed, isotropic=loss == "fd-isotropic", fp64=fp64)
     else:
         raise ValueError(f"unknown loss {loss!r}")
-    go, gm = coded_backward(g, xf, sensor, amp, coded_surface, transfer_1, transfer_2, shifts_xy,
-                            downsample, workers)
-    return loss, go, gm
+    out = coded_backward(g, xf, sensor, amp, coded_surface, transfer_1, transfer_2, shifts_xy,
+                         downsample, workers, with_shifts=with_shifts)
+    return (loss, *out)
 
 
 def nearfield_sweep(object_field, probe_field, transfer, shifts_xy, downsample, measured_u16, scale,

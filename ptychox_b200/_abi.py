@@ -57,6 +57,8 @@ SIGNATURES: dict[str, tuple] = {
     "ptx_coded_sweep": (_i, [_p, _p, _p, _p, _i, _p, _i, _i, _p, _f, _p, _p, _p, _p, _sz, _p]),
     "ptx_coded_fd_workspace_bytes": (_sz, [_i, _i, _i]),
     "ptx_coded_sweep_fd": (_i, [_p, _p, _p, _p, _i, _p, _i, _i, _p, _f, _i, _p, _p, _p, _p, _sz, _p]),
+    "ptx_coded_sweep_ex_workspace_bytes": (_sz, [_i, _i, _i, _i]),
+    "ptx_coded_sweep_ex": (_i, [_p, _p, _p, _p, _i, _p, _i, _i, _p, _f, _i, _p, _p, _p, _p, _p, _sz, _p]),
     "ptx_adam_step": (_i, [_p, _p, _p, _p, _sz, _p, _f, _f, _f, _f, _i, _p]),
     "ptx_base_sweep_noalloc": (_i, [_p, _i, _i, _p, _i, _i, _p, _i, _p, _f, _p, _p, _p, _p]),
 }

@@ -165,8 +165,9 @@ nearfield_ptychography = ptychoX_nearfield
 LOSSES = ("mse", "fd-isotropic", "fd-anisotropic")
 
 
-def coded_sweep(obj, mask, t1, t2, shifts, downsample, measured, scale, ws=None, loss="mse"):
-    """One fused coded (or near-field, ``t1=None``) sweep; returns ``(loss, grad_object, grad_mask)``.
+def coded_sweep(obj, mask, t1, t2, shifts, downsample, measured, scale, ws=None, loss="mse", with_shifts=False):
+    """One fused coded (or near-field, ``t1=None``) sweep; returns ``(loss, grad_object, grad_mask)``,
+    plus the FP64 gradient w.r.t. the shifts (``[batch, 2]``) when ``with_shifts``.
 
     ``loss``: ``"mse"`` (``F.mse_loss``) or the periodic finite-difference loss of
     ``train_coded.py:101-107`` (``"fd-isotropic"`` / ``"fd-anisotropic"``).
@@ -178,6 +179,16 @@ def coded_sweep(obj, mask, t1, t2, shifts, downsample, measured, scale, ws=None,
     out = torch.empty((), dtype=torch.float64, device=dev)
     go = torch.empty_like(obj)
     gm = torch.empty_like(mask)
+    if with_shifts:
+        kind = LOSSES.index(loss)  # PTX_LOSS_MSE / _FD_ISOTROPIC / _FD_ANISOTROPIC
+        gs = torch.empty((batch, 2), dtype=torch.float64, device=dev)
+        if ws is None:
+            ws = workspace(_abi.query("ptx_coded_sweep_ex_workspace_bytes", n, batch, int(downsample), kind), dev)
+        with torch.cuda.device(dev):
+            _abi.call("ptx_coded_sweep_ex", ptr(obj), ptr(mask), ptr(t1), ptr(t2), n, ptr(shifts), batch,
+                      int(downsample), ptr(measured), float(scale), kind, ptr(out), ptr(go), ptr(gm), ptr(gs),
+                      ptr(ws), ws.numel(), stream_handle(dev))
+        return out, go, gm, gs
     with torch.cuda.device(dev):
         if loss == "mse":
             if ws is None:
@@ -204,15 +215,26 @@ class PtychoXCodedLossFunction(torch.autograd.Function):
         meas = as_u16(measured, obj.device)
         if tuple(meas.shape) != (shifts.shape[0], n // ds, n // ds):
             raise ValueError("measured must have shape [batch, H/downsample, W/downsample].")
-        value, go, gm = coded_sweep(obj, mask, t1, t2, shifts, ds, meas, scale, loss=loss)
-        ctx.save_for_backward(go, gm)
+        ctx.shift_dtype = shifts_xy.dtype if torch.is_tensor(shifts_xy) else torch.float32
+        ctx.shift_device = shifts_xy.device if torch.is_tensor(shifts_xy) else obj.device
+        if ctx.needs_input_grad[4]:
+            # position refinement: the shifts enter through the phase ramp only
+            value, go, gm, gs = coded_sweep(obj, mask, t1, t2, shifts, ds, meas, scale, loss=loss, with_shifts=True)
+            ctx.save_for_backward(go, gm, gs)
+        else:
+            value, go, gm = coded_sweep(obj, mask, t1, t2, shifts, ds, meas, scale, loss=loss)
+            ctx.save_for_backward(go, gm)
         return value
 
     @staticmethod
     def backward(ctx, grad_loss):  # type: ignore[override]
-        go, gm = ctx.saved_tensors
+        saved = ctx.saved_tensors
+        go, gm = saved[0], saved[1]
         g = grad_loss.to(torch.float32)
-        return go * g, gm * g, None, None, None, None, None, None, None
+        g_shift = None
+        if len(saved) == 3:
+            g_shift = (saved[2] * grad_loss.to(torch.float64)).to(device=ctx.shift_device, dtype=ctx.shift_dtype)
+        return go * g, gm * g, None, None, g_shift, None, None, None, None
 
 
 def ptychoX_coded_loss(object_field, coded_surface, transfer_1, transfer_2, shifts_xy, downsample, measured,

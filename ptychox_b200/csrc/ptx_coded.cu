@@ -58,7 +58,7 @@ template <int STAGE, bool CONJ, int N>
 __global__ void __launch_bounds__(256, 2) coded_cols(
     float2* __restrict__ scratch, const float2* __restrict__ ospec, const float2* __restrict__ t1,
     const float2* __restrict__ t2, const float* __restrict__ shifts, float inv_n, float2* __restrict__ grad_ospec,
-    const float2* __restrict__ tw) {
+    const float2* __restrict__ tw, double* __restrict__ grad_shifts) {
   using S = RegShape<N>;
   using CP = ColPass<N>;
   extern __shared__ float2 sm[];
@@ -107,6 +107,9 @@ __global__ void __launch_bounds__(256, 2) coded_cols(
       }
       reg_fft<N, true, true>(v, buf, t, tw);
     } else {  // STAGE 7
+      // with grad_shifts: dL/d(dx, dy) += -2 pi sum (fx, fy) Im(conj(G) u), G = v / n the
+      // gradient of u = O^ T1 R (the ramp is the only place the shifts enter)
+      float sx = 0.f, sy = 0.f;
       if (col_ok) {
 #pragma unroll
         for (int m = 0; m < S::N1; ++m) {
@@ -114,8 +117,20 @@ __global__ void __launch_bounds__(256, 2) coded_cols(
           const size_t idx = (size_t)kr * N + kc;
           float2 w = shift_ramp(dx, dy, fx, signed_freq(kr, N));
           if (t1) w = cmul(w, t1[idx]);
-          atomicAdd(&grad_ospec[idx], cmulc(cscale(v[m], inv_n), w));
+          const float2 G = cscale(v[m], inv_n);
+          atomicAdd(&grad_ospec[idx], cmulc(G, w));
+          if (grad_shifts) {
+            const float2 u = cmul(ospec[idx], w);
+            const float im = fmaf(G.x, u.y, -G.y * u.x);  // Im(conj(G) u)
+            sx = fmaf(static_cast<float>(fx), im, sx);
+            sy = fmaf(static_cast<float>(signed_freq(kr, N)), im, sy);
+          }
         }
+      }
+      if (grad_shifts) {
+        constexpr double kTwoPi = 6.283185307179586476925286766559;
+        block_add_double(static_cast<double>(sx), -kTwoPi, &grad_shifts[2 * f]);
+        block_add_double(static_cast<double>(sy), -kTwoPi, &grad_shifts[2 * f + 1]);
       }
       return;
     }
@@ -642,7 +657,7 @@ void launch_fft2(const float2* in, int n, float2* out, float2* tmp, const LinePl
 
 template <int STAGE, bool CONJ>
 void launch_cols(const CodedGeom& g, int nf, const float2* t1, const float2* t2, const float* shifts,
-                 cudaStream_t s) {
+                 cudaStream_t s, double* grad_shifts = nullptr) {
   const float inv_n = 1.0f / static_cast<float>((double)g.n * g.n);
   prof_begin(kCodedCols, s);
   dispatch_pow2(g.n, [&](auto NT) {
@@ -659,7 +674,7 @@ void launch_cols(const CodedGeom& g, int nf, const float2* t1, const float2* t2,
     }
     dim3 grid(num_tiles(N) * (kTile / kColsPerCta), nf);
     coded_cols<STAGE, CONJ, N><<<grid, ColPass<N>::kThreads, kColsPerCta * ColPass<N>::LP * (int)sizeof(float2), s>>>(
-        g.frames, g.ospec, t1, t2, shifts, inv_n, g.gospec, g.plan.tw);
+        g.frames, g.ospec, t1, t2, shifts, inv_n, g.gospec, g.plan.tw, STAGE == 7 ? grad_shifts : nullptr);
   });
   prof_end(kCodedCols, s);
 }
@@ -713,16 +728,56 @@ void launch_rows_grad_mask(const CodedGeom& g, int nf, const float2* mask, const
 
 // The adjoint passes 4 (backward part) to 7 for one chunk, given g_s already in the frames.
 void adjoint_tail(const CodedGeom& g, int nf, const float2* mask, const float2* t1, const float2* t2,
-                  const float* shifts, const float2* xstore, float2* grad_mask, cudaStream_t s) {
+                  const float* shifts, const float2* xstore, float2* grad_mask, cudaStream_t s,
+                  double* grad_shifts = nullptr) {
   launch_cols<3, true>(g, nf, t1, t2, shifts, s);
   launch_rows_grad_mask(g, nf, mask, xstore, grad_mask, s);
-  launch_cols<7, false>(g, nf, t1, t2, shifts, s);
+  launch_cols<7, false>(g, nf, t1, t2, shifts, s, grad_shifts);
 }
 
 }  // namespace
 }  // namespace ptx
 
 using namespace ptx;
+
+namespace ptx {
+namespace {
+int coded_backward_impl(const float* grad_output, const float* x_forward, const float* sensor, const float* amplitude,
+                        const float* coded_surface, const float* transfer_1, const float* transfer_2, int n,
+                        const float* shifts_xy, int batch, int downsample, float* grad_object, float* grad_coded,
+                        void* workspace, size_t workspace_bytes, void* stream, double* grad_shifts) {
+  CodedGeom g;
+  if (int st = coded_check(n, downsample, coded_surface, coded_surface, transfer_2, shifts_xy, batch, workspace,
+                           workspace_bytes, false, &g)) {
+    return st;
+  }
+  if (((!grad_output || !x_forward || !sensor || !amplitude) && batch > 0) || !grad_object || !grad_coded) {
+    return set_error(PTX_ERR_INVALID_ARGUMENT, "null pointer argument");
+  }
+  if (reinterpret_cast<uintptr_t>(x_forward) & 15) {
+    return set_error(PTX_ERR_INVALID_ARGUMENT, "x_forward must be 16-byte aligned");
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const float2* T1 = reinterpret_cast<const float2*>(transfer_1);
+  const float2* T2 = reinterpret_cast<const float2*>(transfer_2);
+  const float2* M = reinterpret_cast<const float2*>(coded_surface);
+  cudaMemsetAsync(g.gospec, 0, g.field_bytes, s);
+  cudaMemsetAsync(grad_coded, 0, g.field_bytes, s);
+  for (int b0 = 0; b0 < batch; b0 += g.chunk) {
+    const int nf = std::min(g.chunk, batch - b0);
+    launch_rows_pool<kCodedBackward>(g, b0, nf, nullptr, 0.f, 0.f, 0.0, nullptr,
+                                     const_cast<float2*>(reinterpret_cast<const float2*>(sensor)),
+                                     const_cast<float*>(amplitude), grad_output, s);
+    adjoint_tail(g, nf, M, T1, T2, shifts_xy + 2 * (size_t)b0,
+                 reinterpret_cast<const float2*>(x_forward) + (size_t)b0 * n * n,
+                 reinterpret_cast<float2*>(grad_coded), s, grad_shifts ? grad_shifts + 2 * (size_t)b0 : nullptr);
+  }
+  launch_fft2<true>(g.gospec, n, reinterpret_cast<float2*>(grad_object), g.tmp, g.plan, s);
+  return cuda_status(cudaGetLastError(), "ptx_coded_backward launch");
+}
+
+}  // namespace
+}  // namespace ptx
 
 extern "C" {
 
@@ -763,40 +818,15 @@ int ptx_coded_backward(const float* grad_output, const float* x_forward, const f
                        const float* coded_surface, const float* transfer_1, const float* transfer_2, int n,
                        const float* shifts_xy, int batch, int downsample, float* grad_object, float* grad_coded,
                        void* workspace, size_t workspace_bytes, void* stream) {
-  CodedGeom g;
-  if (int st = coded_check(n, downsample, coded_surface, coded_surface, transfer_2, shifts_xy, batch, workspace,
-                           workspace_bytes, false, &g)) {
-    return st;
-  }
-  if (((!grad_output || !x_forward || !sensor || !amplitude) && batch > 0) || !grad_object || !grad_coded) {
-    return set_error(PTX_ERR_INVALID_ARGUMENT, "null pointer argument");
-  }
-  if (reinterpret_cast<uintptr_t>(x_forward) & 15) {
-    return set_error(PTX_ERR_INVALID_ARGUMENT, "x_forward must be 16-byte aligned");
-  }
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const float2* T1 = reinterpret_cast<const float2*>(transfer_1);
-  const float2* T2 = reinterpret_cast<const float2*>(transfer_2);
-  const float2* M = reinterpret_cast<const float2*>(coded_surface);
-  cudaMemsetAsync(g.gospec, 0, g.field_bytes, s);
-  cudaMemsetAsync(grad_coded, 0, g.field_bytes, s);
-  for (int b0 = 0; b0 < batch; b0 += g.chunk) {
-    const int nf = std::min(g.chunk, batch - b0);
-    launch_rows_pool<kCodedBackward>(g, b0, nf, nullptr, 0.f, 0.f, 0.0, nullptr,
-                                     const_cast<float2*>(reinterpret_cast<const float2*>(sensor)),
-                                     const_cast<float*>(amplitude), grad_output, s);
-    adjoint_tail(g, nf, M, T1, T2, shifts_xy + 2 * (size_t)b0,
-                 reinterpret_cast<const float2*>(x_forward) + (size_t)b0 * n * n,
-                 reinterpret_cast<float2*>(grad_coded), s);
-  }
-  launch_fft2<true>(g.gospec, n, reinterpret_cast<float2*>(grad_object), g.tmp, g.plan, s);
-  return cuda_status(cudaGetLastError(), "ptx_coded_backward launch");
+  return coded_backward_impl(grad_output, x_forward, sensor, amplitude, coded_surface, transfer_1, transfer_2, n,
+                             shifts_xy, batch, downsample, grad_object, grad_coded, workspace, workspace_bytes, stream,
+                             nullptr);
 }
 
-int ptx_coded_sweep(const float* object, const float* coded_surface, const float* transfer_1, const float* transfer_2,
-                    int n, const float* shifts_xy, int batch, int downsample, const uint16_t* measured, float scale,
-                    double* loss, float* grad_object, float* grad_coded, void* workspace, size_t workspace_bytes,
-                    void* stream) {
+static int coded_sweep_mse(const float* object, const float* coded_surface, const float* transfer_1,
+                           const float* transfer_2, int n, const float* shifts_xy, int batch, int downsample,
+                           const uint16_t* measured, float scale, double* loss, float* grad_object, float* grad_coded,
+                           double* grad_shifts, void* workspace, size_t workspace_bytes, void* stream) {
   CodedGeom g;
   if (int st = coded_check(n, downsample, object, coded_surface, transfer_2, shifts_xy, batch, workspace,
                            workspace_bytes, true, &g)) {
@@ -815,6 +845,7 @@ int ptx_coded_sweep(const float* object, const float* coded_surface, const float
     prof_begin(kMiscKernel, s);
     sweep_prologue_kernel<<<prologue_blocks(nf, sm_count()), 256, 0, s>>>(
         g.gospec, nf, reinterpret_cast<float2*>(grad_coded), nf, loss, nullptr, nullptr, 0.f);
+    if (grad_shifts) cudaMemsetAsync(grad_shifts, 0, sizeof(double) * 2 * (size_t)batch, s);
     prof_end(kMiscKernel, s);
   }
   const int lw = n / downsample;
@@ -829,12 +860,21 @@ int ptx_coded_sweep(const float* object, const float* coded_surface, const float
     launch_cols<3, false>(g, nf, T1, T2, sh, s);
     launch_rows_pool<kCodedSweep>(g, b0, nf, measured, scale, grad_scale, 1.0 / std::max(numel, 1.0), loss, nullptr,
                                   nullptr, nullptr, s);
-    adjoint_tail(g, nf, M, T1, T2, sh, g.xstore, reinterpret_cast<float2*>(grad_coded), s);
+    adjoint_tail(g, nf, M, T1, T2, sh, g.xstore, reinterpret_cast<float2*>(grad_coded), s,
+                 grad_shifts ? grad_shifts + 2 * (size_t)b0 : nullptr);
   }
   launch_fft2<true>(g.gospec, n, reinterpret_cast<float2*>(grad_object), g.tmp, g.plan, s);
   return cuda_status(cudaGetLastError(), "ptx_coded_sweep launch");
 }
 
+
+int ptx_coded_sweep(const float* object, const float* coded_surface, const float* transfer_1, const float* transfer_2,
+                    int n, const float* shifts_xy, int batch, int downsample, const uint16_t* measured, float scale,
+                    double* loss, float* grad_object, float* grad_coded, void* workspace, size_t workspace_bytes,
+                    void* stream) {
+  return coded_sweep_mse(object, coded_surface, transfer_1, transfer_2, n, shifts_xy, batch, downsample, measured,
+                         scale, loss, grad_object, grad_coded, nullptr, workspace, workspace_bytes, stream);
+}
 
 size_t ptx_coded_fd_workspace_bytes(int n, int batch, int downsample) {
   if (n <= 0 || batch < 0 || downsample <= 0) return 0;
@@ -845,10 +885,11 @@ size_t ptx_coded_fd_workspace_bytes(int n, int batch, int downsample) {
   return 2 * up(b * field) + 2 * up(b * pooled) + ptx_coded_workspace_bytes(n, batch);
 }
 
-int ptx_coded_sweep_fd(const float* object, const float* coded_surface, const float* transfer_1,
-                       const float* transfer_2, int n, const float* shifts_xy, int batch, int downsample,
-                       const uint16_t* measured, float scale, int isotropic, double* loss, float* grad_object,
-                       float* grad_coded, void* workspace, size_t workspace_bytes, void* stream) {
+static int coded_sweep_fd(const float* object, const float* coded_surface, const float* transfer_1,
+                          const float* transfer_2, int n, const float* shifts_xy, int batch, int downsample,
+                          const uint16_t* measured, float scale, int isotropic, double* loss, float* grad_object,
+                          float* grad_coded, double* grad_shifts, void* workspace, size_t workspace_bytes,
+                          void* stream) {
   if (!loss || !grad_object || !grad_coded || !workspace || (!measured && batch > 0)) {
     return set_error(PTX_ERR_INVALID_ARGUMENT, "null pointer argument");
   }
@@ -891,8 +932,43 @@ int ptx_coded_sweep_fd(const float* object, const float* coded_surface, const fl
                                                                             isotropic, gamp, loss);
     prof_end(kMiscKernel, s);
   }
-  return ptx_coded_backward(gamp, xf, sensor, amp, coded_surface, transfer_1, transfer_2, n, shifts_xy, batch,
-                            downsample, grad_object, grad_coded, p, inner, stream);
+  // the backward reuses the forward's region of the workspace, whose object spectrum the
+  // shift gradient reads
+  if (grad_shifts) cudaMemsetAsync(grad_shifts, 0, sizeof(double) * 2 * (size_t)batch, s);
+  return coded_backward_impl(gamp, xf, sensor, amp, coded_surface, transfer_1, transfer_2, n, shifts_xy, batch,
+                             downsample, grad_object, grad_coded, p, inner, stream, grad_shifts);
+}
+
+int ptx_coded_sweep_fd(const float* object, const float* coded_surface, const float* transfer_1,
+                       const float* transfer_2, int n, const float* shifts_xy, int batch, int downsample,
+                       const uint16_t* measured, float scale, int isotropic, double* loss, float* grad_object,
+                       float* grad_coded, void* workspace, size_t workspace_bytes, void* stream) {
+  return coded_sweep_fd(object, coded_surface, transfer_1, transfer_2, n, shifts_xy, batch, downsample, measured,
+                        scale, isotropic, loss, grad_object, grad_coded, nullptr, workspace, workspace_bytes, stream);
+}
+
+size_t ptx_coded_sweep_ex_workspace_bytes(int n, int batch, int downsample, int loss_kind) {
+  return loss_kind == PTX_LOSS_MSE ? ptx_coded_workspace_bytes(n, batch)
+                                   : ptx_coded_fd_workspace_bytes(n, batch, downsample);
+}
+
+int ptx_coded_sweep_ex(const float* object, const float* coded_surface, const float* transfer_1,
+                       const float* transfer_2, int n, const float* shifts_xy, int batch, int downsample,
+                       const uint16_t* measured, float scale, int loss_kind, double* loss, float* grad_object,
+                       float* grad_coded, double* grad_shifts, void* workspace, size_t workspace_bytes, void* stream) {
+  switch (loss_kind) {
+    case PTX_LOSS_MSE:
+      return coded_sweep_mse(object, coded_surface, transfer_1, transfer_2, n, shifts_xy, batch, downsample,
+                             measured, scale, loss, grad_object, grad_coded, grad_shifts, workspace, workspace_bytes,
+                             stream);
+    case PTX_LOSS_FD_ISOTROPIC:
+    case PTX_LOSS_FD_ANISOTROPIC:
+      return coded_sweep_fd(object, coded_surface, transfer_1, transfer_2, n, shifts_xy, batch, downsample,
+                            measured, scale, loss_kind == PTX_LOSS_FD_ISOTROPIC ? 1 : 0, loss, grad_object,
+                            grad_coded, grad_shifts, workspace, workspace_bytes, stream);
+    default:
+      return set_error(PTX_ERR_INVALID_ARGUMENT, "unknown loss kind %d", loss_kind);
+  }
 }
 
 }  // extern "C"

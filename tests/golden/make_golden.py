@@ -158,6 +158,42 @@ def sweep_coded(ptychoX, name, n, ds, count, photons, seed, nearfield, loss_fn=N
              nearfield=nearfield)
 
 
+def shift_case(ptychoX):
+    """Gradient w.r.t. the coded shifts: the reference's torch formulation
+    (``coded/ops.py:136-171``, differentiable in ``shifts_xy`` through ``shift_phase_ramp``)
+    in complex128 with the MSE loss, written with every gradient."""
+    from ptychoX.coded.ops import _coded_forward_torch
+
+    n, ds, count, photons, seed = 32, 2, 4, 200.0, 17
+    rng = np.random.default_rng(seed)
+    obj_true = synth.random_object(n, n, rng)
+    mask = synth.binary_mask(n, 0.5, rng)
+    dx = 1.85e-6
+    t2 = synth.angular_spectrum_transfer(n, dx, 0.5e-6, 2e-3)
+    t1 = synth.angular_spectrum_transfer(n, dx, 0.5e-6, 396.95e-6)
+    shifts = synth.coded_shifts(count, 3.0, n, rng)
+    t1_t = torch.from_numpy(t1.astype(np.complex128))
+    t2_t = torch.from_numpy(t2.astype(np.complex128))
+    with torch.no_grad():
+        amp = _coded_forward_torch(torch.from_numpy(obj_true.astype(np.complex128)),
+                                   torch.from_numpy(mask.astype(np.complex128)), t1_t, t2_t,
+                                   torch.from_numpy(shifts.astype(np.float64)), ds)[3]
+    counts, scale = synth.poisson_counts(_np(amp) ** 2, photons, rng, per_pixel=True)
+    obj = (obj_true * (1.0 + 0.15 * rng.standard_normal(obj_true.shape))).astype(np.complex64)
+    msk = (mask * (1.0 + 0.1 * rng.standard_normal(mask.shape)) + 0.05).astype(np.complex64)
+    # evaluate with shifts off by up to 0.3 px so the shift gradient is far from zero
+    sh_eval = (shifts + rng.uniform(-0.3, 0.3, shifts.shape) / n).astype(np.float32)
+    o = torch.from_numpy(obj.astype(np.complex128)).requires_grad_(True)
+    m = torch.from_numpy(msk.astype(np.complex128)).requires_grad_(True)
+    sh = torch.from_numpy(sh_eval.astype(np.float64)).requires_grad_(True)
+    pred = _coded_forward_torch(o, m, t1_t, t2_t, sh, ds)[3]
+    loss = F.mse_loss(pred, _observed(counts, scale))
+    loss.backward()
+    np.savez(HERE / "sweep_coded_shifts_fp64.npz", object=obj, mask=msk, transfer_1=t1, transfer_2=t2,
+             shifts=sh_eval, downsample=ds, measured=counts, scale=np.float32(scale), loss=float(loss.item()),
+             grad_object=_np(o.grad), grad_mask=_np(m.grad), grad_shifts=_np(sh.grad))
+
+
 def fd_cases(ptychoX):
     import train_coded  # the reference's coded training driver (defines fd_loss)
 
@@ -178,15 +214,16 @@ def main(ref_python_dir: str) -> None:
     sweep_coded(ptychoX, "sweep_coded_fp64.npz", 32, 2, 4, 200.0, seed=14, nearfield=False)
     sweep_coded(ptychoX, "sweep_nearfield_fp64.npz", 32, 4, 3, 200.0, seed=15, nearfield=True)
     fd_cases(ptychoX)
+    shift_case(ptychoX)
     print("wrote", sorted(p.name for p in HERE.glob("*.npz")))
 
 
 if __name__ == "__main__":
-    if len(sys.argv) > 2 and sys.argv[2] == "fd":  # only the fd_loss fixtures
+    if len(sys.argv) > 2 and sys.argv[2] in ("fd", "shifts"):  # only the fd_loss / shift fixtures
         sys.dont_write_bytecode = True
         sys.path.insert(0, sys.argv[1])
         import ptychoX  # noqa: E402
 
-        fd_cases(ptychoX)
+        fd_cases(ptychoX) if sys.argv[2] == "fd" else shift_case(ptychoX)
     else:
         main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/python")

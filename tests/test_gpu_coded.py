@@ -173,3 +173,44 @@ def test_fd_loss_vs_oracle_and_autograd(nearfield, loss):
     assert abs(float(val.item()) - loss_v) <= 1e-12 * abs(loss_v)
     assert rel_l2(o.grad.cpu().numpy(), go) < 1e-6 and rel_l2(m.grad.cpu().numpy(), gm) < 1e-6
 
+
+def test_shift_gradient_golden():
+    """Position refinement: dL/dshifts against autograd through the reference's torch
+    formulation (coded/ops.py:157-171), with the object and mask gradients of the same sweep."""
+    from ptychox_b200.coded import coded_sweep
+
+    g = load_golden("sweep_coded_shifts_fp64.npz")
+    args = (g["object"], g["mask"], g["transfer_1"], g["transfer_2"], g["shifts"], int(g["downsample"]),
+            g["measured"], float(g["scale"]))
+    loss, go, gm, gs = coded_sweep(cuda(g["object"]), cuda(g["mask"]), cuda(g["transfer_1"]), cuda(g["transfer_2"]),
+                                   cuda(g["shifts"].astype(np.float32)), int(g["downsample"]), cuda(g["measured"]),
+                                   float(g["scale"]), with_shifts=True)
+    torch.cuda.synchronize()
+    ref = O.coded_sweep(*args, fp64=False, with_shifts=True)
+    assert abs(float(loss.item()) - float(g["loss"])) <= TOL * abs(float(g["loss"]))
+    assert rel_l2(go.cpu().numpy(), g["grad_object"]) < fp32_tol(rel_l2(ref[1], g["grad_object"]))
+    assert rel_l2(gm.cpu().numpy(), g["grad_mask"]) < fp32_tol(rel_l2(ref[2], g["grad_mask"]))
+    assert rel_l2(gs.cpu().numpy(), g["grad_shifts"]) < fp32_tol(rel_l2(ref[3], g["grad_shifts"]))
+
+
+@pytest.mark.parametrize("loss", ["mse", "fd-isotropic"])
+def test_shift_gradient_autograd_and_oracle(loss):
+    """128^2 field, 6 shifts, ds 2: shifts_xy.requires_grad through ptychoX_coded_loss gives
+    the FP64 oracle's shift gradient (MSE and fd_loss), and leaves the other gradients as the
+    sweep without shifts."""
+    from ptychox_b200 import ptychoX_coded_loss
+
+    obj, mask, t1, t2, shifts, meas, scale = coded_problem(128, 6, 8.0, 2, 500.0, seed=23, nearfield=False)
+    shifts = (shifts + np.random.default_rng(1).uniform(-0.3, 0.3, shifts.shape) / 128).astype(np.float32)
+    ref = O.coded_sweep(obj, mask, t1, t2, shifts, 2, meas, scale, loss=loss, with_shifts=True)
+    ref32 = O.coded_sweep(obj, mask, t1, t2, shifts, 2, meas, scale, fp64=False, loss=loss, with_shifts=True)
+    o = cuda(obj).requires_grad_(True)
+    m = cuda(mask).requires_grad_(True)
+    sh = torch.from_numpy(shifts).requires_grad_(True)  # a CPU leaf, as a training script may hold it
+    val = ptychoX_coded_loss(o, m, cuda(t1), cuda(t2), sh, 2, cuda(meas), scale, loss=loss)
+    val.backward()
+    assert sh.grad is not None and sh.grad.dtype == torch.float32 and sh.grad.device.type == "cpu"
+    assert rel_l2(sh.grad.numpy().astype(np.float64), ref[3]) < fp32_tol(rel_l2(ref32[3], ref[3]))
+    assert rel_l2(o.grad.cpu().numpy(), ref[1]) < fp32_tol(rel_l2(ref32[1], ref[1]))
+    assert rel_l2(m.grad.cpu().numpy(), ref[2]) < fp32_tol(rel_l2(ref32[2], ref[2]))
+

@@ -94,3 +94,15 @@ def test_sweep_coded_fd_loss(name, loss):
     assert abs(got - float(g["loss"])) <= TOL_F64 * abs(float(g["loss"]))
     assert rel_l2(go, g["grad_object"]) < TOL_F64
     assert rel_l2(gm, g["grad_mask"]) < TOL_F64
+
+
+def test_coded_shift_gradient():
+    """dL/dshifts: the reference's torch formulation is differentiable in shifts_xy through
+    shift_phase_ramp (coded/ops.py:157-171); the oracle's closed form matches its autograd."""
+    g = load_golden("sweep_coded_shifts_fp64.npz")
+    loss, go, gm, gs = O.coded_sweep(g["object"], g["mask"], g["transfer_1"], g["transfer_2"], g["shifts"],
+                                     int(g["downsample"]), g["measured"], float(g["scale"]), with_shifts=True)
+    assert abs(loss - float(g["loss"])) <= TOL_F64 * abs(float(g["loss"]))
+    assert rel_l2(go, g["grad_object"]) < TOL_F64
+    assert rel_l2(gm, g["grad_mask"]) < TOL_F64
+    assert rel_l2(gs, g["grad_shifts"]) < TOL_F64
