@@ -519,39 +519,82 @@ def run_ours(args) -> None:
     }
 
     # ---- e2e: public API with pinned host buffers -----------------------------------
+    # A training loop as a user writes it against the public API, with each step's inputs
+    # uploaded from pinned host memory and its loss and gradients read back.  The copies run on
+    # two copy streams with double-buffered device inputs, so step k+1's upload and step k-1's
+    # read-back overlap step k's sweep (PCIe is full duplex).  Timed from the first upload to
+    # the last read-back on the device.
     host = prob["host"]
     h_obj = torch.from_numpy(host["obj"]).pin_memory()
     h_aux = torch.from_numpy(host["aux"]).pin_memory()
     h_pos = torch.from_numpy(host["pos"]).pin_memory()
-    out_go = torch.empty_like(h_obj).pin_memory()
-    out_ga = torch.empty_like(h_aux).pin_memory()
-    out_loss = torch.empty((), dtype=torch.float64).pin_memory()
+    out_go = [torch.empty_like(h_obj).pin_memory() for _ in range(2)]
+    out_ga = [torch.empty_like(h_aux).pin_memory() for _ in range(2)]
+    out_loss = [torch.empty((), dtype=torch.float64).pin_memory() for _ in range(2)]
+    d_in = [(torch.empty_like(h_obj, device=dev), torch.empty_like(h_aux, device=dev)) for _ in range(2)]
+    s_comp = torch.cuda.current_stream(dev)
+    s_up = torch.cuda.Stream(device=dev)
+    s_down = torch.cuda.Stream(device=dev)
 
-    def e2e_step():
-        d_obj = h_obj.to(dev, non_blocking=True).requires_grad_(True)
-        d_aux = h_aux.to(dev, non_blocking=True).requires_grad_(True)
-        d_pos = h_pos.to(dev, non_blocking=True)
-        loss = wl.loss_api(d_obj, d_aux, d_pos, prob)
-        loss.backward()
-        if world > 1:
-            reduce_sweep(loss.detach(), [d_obj.grad, d_aux.grad], wl.batch, wl.batch * world)
-        out_go.copy_(d_obj.grad, non_blocking=True)
-        out_ga.copy_(d_aux.grad, non_blocking=True)
-        out_loss.copy_(loss.detach(), non_blocking=True)
+    def upload(b):
+        with torch.cuda.stream(s_up):
+            for d, h in zip(d_in[b], (h_obj, h_aux)):
+                d.copy_(h, non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(s_up)
+        return ev
 
-    for _ in range(max(1, args.warmup)):
-        e2e_step()
-    torch.cuda.synchronize(dev)
+    def e2e_run(k: int) -> float:
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        start.record(s_up)
+        ready = [upload(0), None]
+        freed = [None, None]  # the compute stream is done with buffer b
+        for i in range(k):
+            b = i & 1
+            if i + 1 < k:
+                if freed[b ^ 1] is not None:
+                    s_up.wait_event(freed[b ^ 1])
+                ready[b ^ 1] = upload(b ^ 1)
+            s_comp.wait_event(ready[b])
+            d_obj = d_in[b][0].detach().requires_grad_(True)
+            d_aux = d_in[b][1].detach().requires_grad_(True)
+            # the scan goes in as pinned host memory: the API checks it on the host and uploads it
+            loss = wl.loss_api(d_obj, d_aux, h_pos, prob)
+            loss.backward()
+            g_obj, g_aux, l_det = d_obj.grad, d_aux.grad, loss.detach()
+            if world > 1:
+                reduce_sweep(l_det, [g_obj, g_aux], wl.batch, wl.batch * world)
+            done = torch.cuda.Event()
+            done.record(s_comp)
+            freed[b] = done
+            s_down.wait_event(done)
+            with torch.cuda.stream(s_down):
+                out_go[b].copy_(g_obj, non_blocking=True)
+                out_ga[b].copy_(g_aux, non_blocking=True)
+                out_loss[b].copy_(l_det, non_blocking=True)
+            for t in (g_obj, g_aux, l_det):
+                t.record_stream(s_down)  # keep the memory until the read-back has finished
+        s_up.wait_stream(s_down)
+        s_up.wait_stream(s_comp)
+        end.record(s_up)
+        torch.cuda.synchronize(dev)
+        return start.elapsed_time(end)
+
+    e2e_run(max(2, args.warmup))
     if world > 1:
         dist.barrier()
-    e2e_ms = max_over_ranks(sum(timed(args.steps, e2e_step)))
+    e2e_ms = max_over_ranks(e2e_run(args.steps))
     h2d = (h_obj.numel() + h_aux.numel()) * 8 + h_pos.numel() * h_pos.element_size()
-    d2h = (out_go.numel() + out_ga.numel()) * 8 + 8
+    d2h = (out_go[0].numel() + out_ga[0].numel()) * 8 + 8
     e2e = {"value": world * args.steps / (e2e_ms / 1e3), "unit": "sweeps/s", "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h,
-           "note": "measured counts resident in HBM (uploaded once, as the reference training loop keeps "
-                   "observed amplitudes on the device); object, probe/pupil/mask and positions uploaded and "
-                   "the loss and both gradients read back every step"}
+           "note": "public loss API (autograd); each step uploads object, probe/pupil/mask and scan from pinned "
+                   "host memory (the scan through the API's own pinned upload) and reads back the loss and "
+                   "both gradients, on two copy streams with double-buffered inputs (uploads and read-backs "
+                   "overlap the neighbouring steps' sweeps); "
+                   "measured counts resident in HBM (uploaded once, as the reference training loop keeps "
+                   "observed amplitudes on the device); timed from the first upload to the last read-back"}
 
     # ---- CPU baseline (rank 0, N = 1) --------------------------------------------------
     cpu = None

@@ -63,13 +63,16 @@ def device_positions(
     """
     pos = positions_xy.to(dtype=torch.long)
     if check_bounds and pos.numel():
-        host = pos.detach().cpu()
+        # host positions are checked where they are (no device round trip)
+        host = pos.detach() if pos.device.type == "cpu" else pos.detach().cpu()
         wh, ww = window_hw
         fh, fw = field_hw
         x, y = host[:, 0], host[:, 1]
         if bool((x < 0).any() or (y < 0).any() or (x + ww > fw).any() or (y + wh > fh).any()):
             raise ValueError(f"{name}: a {wh}x{ww} window leaves the {fh}x{fw} field.")
-    return pos.to(device=device).contiguous()
+    # pinned host positions upload asynchronously on the current stream
+    nb = pos.device.type == "cpu" and pos.is_pinned()
+    return pos.to(device=device, non_blocking=nb).contiguous()
 
 
 def stream_handle(device: torch.device) -> int:

@@ -50,7 +50,8 @@ def clear_cuda_plan_cache() -> None:
 def _prepare(object_field, pupil, led_indices_xy):
     check_complex_scan_inputs(object_field, pupil, led_indices_xy, "object_field", "pupil")
     require_cuda_complex64(("object_field", object_field), ("pupil", pupil))
-    led = led_indices_xy.to(device=object_field.device, dtype=torch.long).contiguous()
+    nb = led_indices_xy.device.type == "cpu" and led_indices_xy.is_pinned()  # pinned: asynchronous upload
+    led = led_indices_xy.to(device=object_field.device, dtype=torch.long, non_blocking=nb).contiguous()
     return object_field.contiguous(), pupil.contiguous(), led
 
 
