@@ -687,10 +687,6 @@ int check_common(const void* sample, int H, int W, const void* probe, int ph, in
                      ws_bytes, kHeaderBytes + g->frame_bytes);
   }
   size_t fit = (ws_bytes - kHeaderBytes) / g->frame_bytes;
-  if (const char* env = getenv("PTYCHOX_CHUNK_FRAMES")) {
-    const long v = atol(env);
-    if (v > 0 && (size_t)v < fit) fit = (size_t)v;
-  }
   g->chunk = static_cast<int>(std::min<size_t>(fit, (size_t)std::max(batch, 1)));
   g->err = reinterpret_cast<unsigned*>(ws);
   g->lut = reinterpret_cast<float*>(static_cast<char*>(ws) + 256);
