@@ -255,7 +255,6 @@ __global__ void __launch_bounds__(256) base_rows_adjoint_rt(
 
 template <int N>
 struct RowCfg {
-  static constexpr int T = RegShape<N>::T;
   static constexpr int LP = row_line_pitch<N>();
 };
 
