@@ -552,10 +552,6 @@ def run_ours(args) -> None:
         freed = [None, None]  # the compute stream is done with buffer b
         for i in range(k):
             b = i & 1
-            if i + 1 < k:
-                if freed[b ^ 1] is not None:
-                    s_up.wait_event(freed[b ^ 1])
-                ready[b ^ 1] = upload(b ^ 1)
             s_comp.wait_event(ready[b])
             d_obj = d_in[b][0].detach().requires_grad_(True)
             d_aux = d_in[b][1].detach().requires_grad_(True)
@@ -568,6 +564,12 @@ def run_ours(args) -> None:
             done = torch.cuda.Event()
             done.record(s_comp)
             freed[b] = done
+            # the next step's upload is queued after this step's own (small) scan upload, so the
+            # scan copy never waits behind it on the copy engine
+            if i + 1 < k:
+                if freed[b ^ 1] is not None:
+                    s_up.wait_event(freed[b ^ 1])
+                ready[b ^ 1] = upload(b ^ 1)
             s_down.wait_event(done)
             with torch.cuda.stream(s_down):
                 out_go[b].copy_(g_obj, non_blocking=True)

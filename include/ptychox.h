@@ -65,6 +65,15 @@ long long ptx_launch_count(void);
  * the reference's kernels are one-shot grids. */
 int ptx_set_units_per_cta(int units);
 
+/* Copy `bytes` from host memory `src` (pageable or page-locked) to device memory `dst`
+ * (current device) in stream order on `stream`.  Up to 256 KiB the bytes are copied at the
+ * call into a page-locked ring owned by the library (so `src` may be reused as soon as the
+ * call returns) and a kernel reads them over the bus: a small per-step input such as a scan
+ * is then neither queued on a copy engine behind another stream's large transfer nor
+ * blocking the host as a pageable copy would.  Larger inputs take cudaMemcpyAsync.  No
+ * reference counterpart: the reference moves scans with torch's `.to(device)`. */
+int ptx_stage_host_bytes(void* dst, const void* src, size_t bytes, void* stream);
+
 /* Optional per-kernel CUDA-event timing: when enabled every launch is bracketed by an
  * event pair on its stream.  ptx_profile_read synchronises on the recorded events and
  * returns the accumulated device time and timed launches of one kernel kind

@@ -70,9 +70,29 @@ def device_positions(
         x, y = host[:, 0], host[:, 1]
         if bool((x < 0).any() or (y < 0).any() or (x + ww > fw).any() or (y + wh > fh).any()):
             raise ValueError(f"{name}: a {wh}x{ww} window leaves the {fh}x{fw} field.")
-    # pinned host positions upload asynchronously on the current stream
-    nb = pos.device.type == "cpu" and pos.is_pinned()
-    return pos.to(device=device, non_blocking=nb).contiguous()
+    return upload_small(pos, device, torch.long)
+
+
+def upload_small(t: torch.Tensor, device: torch.device, dtype: torch.dtype) -> torch.Tensor:
+    """``t`` as a contiguous ``dtype`` tensor on ``device``, in order on the current stream.
+
+    A host tensor (converted to ``dtype`` on the host first) goes through
+    ``ptx_stage_host_bytes``: copied into the library's page-locked ring at the call and read
+    by a kernel on the stream, so a per-step scan neither waits on a copy engine behind
+    another stream's large upload nor blocks the host; device tensors are converted in place.
+    """
+    if t.device.type != "cpu" or torch.device(device).type != "cuda":
+        return t.to(device=device, dtype=dtype).contiguous()
+    host = t.detach().to(dtype=dtype).contiguous()
+    out = torch.empty(host.shape, dtype=dtype, device=device)
+    if host.numel():
+        args = (out.data_ptr(), host.data_ptr(), host.numel() * host.element_size())
+        if out.device.index == torch.cuda.current_device():
+            _abi.call("ptx_stage_host_bytes", *args, stream_handle(out.device))
+        else:
+            with torch.cuda.device(out.device):
+                _abi.call("ptx_stage_host_bytes", *args, stream_handle(out.device))
+    return out
 
 
 def stream_handle(device: torch.device) -> int:

@@ -17,7 +17,7 @@ from __future__ import annotations
 import torch
 
 from . import _abi
-from ._utils import as_u16, ptr, stream_handle, workspace
+from ._utils import as_u16, ptr, stream_handle, upload_small, workspace
 
 __all__ = [
     "ptychoX_coded",
@@ -72,8 +72,7 @@ def _prepare(object_field, coded_surface, transfer_1, transfer_2, shifts_xy, dow
     if h != w:
         raise ValueError("coded / near-field fields must be square.")
     dev = object_field.device
-    nb = shifts_xy.device.type == "cpu" and shifts_xy.is_pinned()  # pinned: asynchronous upload
-    shifts = shifts_xy.to(device=dev, dtype=torch.float32, non_blocking=nb).contiguous()
+    shifts = upload_small(shifts_xy, dev, torch.float32)
     t1 = None if transfer_1 is None else transfer_1.contiguous()
     return object_field.contiguous(), coded_surface.contiguous(), t1, transfer_2.contiguous(), shifts
 

@@ -8,6 +8,8 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstring>
+#include <deque>
 #include <cstdarg>
 #include <cstdio>
 #include <algorithm>
@@ -266,9 +268,125 @@ int persistent_grid(const void* kernel, int threads, int smem, long long units) 
   return static_cast<int>(std::max<long long>(1, std::min<long long>(grid, std::max<long long>(units, 1))));
 }
 
+// Device copy of page-locked host memory, read over the bus with loads that never hit a
+// stale cached line of system memory (ld.global.cv).  Grid-stride; 8-byte words when both
+// ends are 8-byte aligned, bytes otherwise.
+__global__ void stage_host_kernel(unsigned char* __restrict__ dst, const unsigned char* __restrict__ src,
+                                  size_t bytes) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const size_t i0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (((reinterpret_cast<uintptr_t>(dst) | reinterpret_cast<uintptr_t>(src)) & 7) == 0) {
+    const size_t n8 = bytes / 8;
+    auto* d8 = reinterpret_cast<unsigned long long*>(dst);
+    const auto* s8 = reinterpret_cast<const unsigned long long*>(src);
+    for (size_t i = i0; i < n8; i += stride) d8[i] = __ldcv(s8 + i);
+    for (size_t i = n8 * 8 + i0; i < bytes; i += stride) dst[i] = __ldcv(src + i);
+  } else {
+    for (size_t i = i0; i < bytes; i += stride) dst[i] = __ldcv(src + i);
+  }
+}
+
+// ---- staging ring for small host inputs -------------------------------------------------
+// One page-locked, device-mapped ring of kStageRingBytes per device.  stage_host copies the
+// caller's bytes into the next span of the ring (the caller may reuse its memory at once),
+// launches stage_host_kernel to read the span into `dst` on the stream and records the
+// span's event after it.  A span is reused only after its event has completed (normally
+// long before the ring wraps round to it; otherwise the host waits on that event).  The
+// whole sequence runs under one lock, so every span in the ring has its event recorded.
+constexpr size_t kStageRingBytes = 1u << 20;
+constexpr size_t kStageMaxBytes = kStageRingBytes / 4;  // larger inputs take cudaMemcpyAsync
+
+struct StageRing {
+  unsigned char* host = nullptr;
+  unsigned char* device = nullptr;
+  size_t head = 0;
+  struct Span {
+    size_t off, len;
+    cudaEvent_t done;
+  };
+  std::deque<Span> live;
+  std::vector<cudaEvent_t> spare;
+};
+std::mutex g_stage_mutex;
+std::map<int, StageRing> g_stage;
+
+// PTX_OK with *staged = false when the ring cannot take the copy (too large, or no ring on
+// this device): the caller copies instead.
+int stage_host(void* dst, const void* src, size_t bytes, cudaStream_t s, bool* staged) {
+  *staged = false;
+  if (bytes > kStageMaxBytes) return PTX_OK;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return cuda_status(cudaGetLastError(), "cudaGetDevice");
+  std::lock_guard<std::mutex> lock(g_stage_mutex);
+  StageRing& r = g_stage[dev];
+  if (!r.host) {
+    void* h = nullptr;
+    if (cudaHostAlloc(&h, kStageRingBytes, cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess) {
+      cudaGetLastError();
+      return PTX_OK;
+    }
+    void* d = nullptr;
+    if (cudaHostGetDevicePointer(&d, h, 0) != cudaSuccess || !d) {
+      cudaGetLastError();
+      cudaFreeHost(h);
+      return PTX_OK;
+    }
+    r.host = static_cast<unsigned char*>(h);
+    r.device = static_cast<unsigned char*>(d);
+  }
+  // retire completed spans from the oldest end, then wait for any live span the new one overlaps
+  while (!r.live.empty()) {
+    if (cudaEventQuery(r.live.front().done) != cudaSuccess) {
+      cudaGetLastError();
+      break;
+    }
+    r.spare.push_back(r.live.front().done);
+    r.live.pop_front();
+  }
+  const size_t off = r.head + bytes > kStageRingBytes ? 0 : r.head;
+  for (const StageRing::Span& sp : r.live) {
+    if (sp.off < off + bytes && off < sp.off + sp.len && cudaEventSynchronize(sp.done) != cudaSuccess) {
+      return cuda_status(cudaGetLastError(), "staging ring wait");
+    }
+  }
+  cudaEvent_t ev = nullptr;
+  if (!r.spare.empty()) {
+    ev = r.spare.back();
+    r.spare.pop_back();
+  } else if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+    return cuda_status(cudaGetLastError(), "cudaEventCreate");
+  }
+  std::memcpy(r.host + off, src, bytes);
+  const size_t words = (bytes + 7) / 8;
+  const unsigned grid = static_cast<unsigned>(std::min<size_t>((words + 255) / 256, 1024));
+  prof_begin(kMiscKernel, s);
+  stage_host_kernel<<<grid, 256, 0, s>>>(static_cast<unsigned char*>(dst), r.device + off, bytes);
+  prof_end(kMiscKernel, s);
+  const cudaError_t launched = cudaGetLastError();
+  const cudaError_t recorded = launched == cudaSuccess ? cudaEventRecord(ev, s) : launched;
+  if (recorded != cudaSuccess) {
+    r.spare.push_back(ev);
+    return cuda_status(recorded, "ptx_stage_host_bytes launch");
+  }
+  r.live.push_back({off, bytes, ev});
+  r.head = (off + bytes + 15) / 16 * 16;
+  *staged = true;
+  return PTX_OK;
+}
+
 }  // namespace ptx
 
 extern "C" {
+
+int ptx_stage_host_bytes(void* dst, const void* src, size_t bytes, void* stream) {
+  if (bytes == 0) return PTX_OK;
+  if (!dst || !src) return ptx::set_error(PTX_ERR_INVALID_ARGUMENT, "null pointer argument");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  bool staged = false;
+  if (int st = ptx::stage_host(dst, src, bytes, s, &staged)) return st;
+  if (staged) return PTX_OK;
+  return ptx::cuda_status(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, s), "ptx_stage_host_bytes copy");
+}
 
 int ptx_set_units_per_cta(int units) {
   if (units < 0) return ptx::set_error(PTX_ERR_INVALID_ARGUMENT, "units per CTA must be >= 0");

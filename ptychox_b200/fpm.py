@@ -12,7 +12,8 @@ from __future__ import annotations
 import torch
 
 from . import _abi
-from ._utils import as_u16, check_complex_scan_inputs, ptr, require_cuda_complex64, stream_handle, workspace
+from ._utils import (as_u16, check_complex_scan_inputs, ptr, require_cuda_complex64, stream_handle, upload_small,
+                     workspace)
 
 __all__ = [
     "ptychoX_fourier",
@@ -50,8 +51,7 @@ def clear_cuda_plan_cache() -> None:
 def _prepare(object_field, pupil, led_indices_xy):
     check_complex_scan_inputs(object_field, pupil, led_indices_xy, "object_field", "pupil")
     require_cuda_complex64(("object_field", object_field), ("pupil", pupil))
-    nb = led_indices_xy.device.type == "cpu" and led_indices_xy.is_pinned()  # pinned: asynchronous upload
-    led = led_indices_xy.to(device=object_field.device, dtype=torch.long, non_blocking=nb).contiguous()
+    led = upload_small(led_indices_xy, object_field.device, torch.long)
     return object_field.contiguous(), pupil.contiguous(), led
 
 
