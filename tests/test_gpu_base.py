@@ -84,6 +84,29 @@ def test_sweep_vs_oracle_sizes(p):
     assert rel_l2(gp, rp) < TOL
 
 
+@pytest.mark.parametrize("ph,pw,n_pos", [(256, 256, 6), (1024, 1024, 3), (64, 128, 9), (128, 64, 9),
+                                         (96, 160, 6), (512, 256, 4)])
+def test_sweep_vs_oracle_large_and_rectangular(ph, pw, n_pos):
+    """The largest compile-time frame (1024 points per line: 32 threads per row line, 256-thread
+    column CTAs), 256-point frames, and rectangular probes whose rows and columns take
+    different line plans (compile-time and runtime) against the FP64 oracle."""
+    from ptychox_b200 import synth
+
+    rng = np.random.default_rng(ph * 7 + pw)
+    h, w = ph + 3 * 24 + 8, pw + 3 * 24 + 8
+    obj = synth.random_object(h, w, rng)
+    probe = synth.gaussian_probe(ph, pw, rng)
+    pos = np.stack([rng.integers(0, w - pw + 1, n_pos), rng.integers(0, h - ph + 1, n_pos)], axis=1).astype(np.int64)
+    amp, _, _ = O.base_forward(obj, probe, pos)
+    meas, scale = synth.poisson_counts(amp**2, 1e4, rng)
+    guess = (obj * (1 + 0.1 * rng.standard_normal(obj.shape))).astype(np.complex64)
+    loss, gs, gp = run_sweep(guess, probe, pos, meas, scale)
+    rl, rs, rp = O.base_sweep(guess, probe, pos, meas, scale)
+    assert abs(loss - rl) <= TOL * abs(rl)
+    assert rel_l2(gs, rs) < TOL
+    assert rel_l2(gp, rp) < TOL
+
+
 def test_config0_sweep_vs_oracle():
     """Config 0 shape: 512x512 object, 128x128 probe, 11x11 raster step 32 with U[-2,2] jitter."""
     obj, probe, pos, meas, scale = small_problem(512, 128, 11, 32, 8, 2, 1e4, seed=0)
