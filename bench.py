@@ -306,19 +306,10 @@ DEFAULT_WORKLOAD = "conventional-900x512-2048"
 
 
 def device_poisson(amp, photons, seed, per_pixel=False, brightest=False):
-    """uint16 Poisson counts of amp^2 / scale on the device (scale as synth.poisson_counts)."""
-    import torch
+    """uint16 Poisson counts of amp^2 / scale on the device (``synth.poisson_counts_device``)."""
+    from ptychox_b200.synth import poisson_counts_device
 
-    inten = amp.double() ** 2
-    sums = inten.flatten(1).sum(dim=1)
-    per_pattern = float(sums.max() if brightest else sums.mean())
-    denom = photons * (inten[0].numel() if per_pixel else 1)
-    scale = float(np.float32(per_pattern / denom))
-    gen = torch.Generator(device=amp.device).manual_seed(seed)
-    counts = torch.poisson(inten / scale, generator=gen)
-    if float(counts.max()) > 65535:
-        raise RuntimeError("synthetic counts saturate uint16")
-    return counts.to(torch.int32).to(torch.uint16), scale
+    return poisson_counts_device(amp, photons, seed, per_pixel=per_pixel, brightest=brightest)
 
 
 # ---------------------------------------------------------------------------------------

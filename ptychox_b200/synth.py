@@ -1,4 +1,5 @@
-"""Seeded synthetic inputs for the four modalities (host side, numpy).
+"""Seeded synthetic inputs for the four modalities (host side, numpy; the measurement
+synthesis also on the device).
 
 The reference drivers build their problems from images on disk (``cameraman512.png``,
 ``I01.bmp``); the workloads here use seeded synthetic objects of the same shapes:
@@ -13,7 +14,10 @@ The reference drivers build their problems from images on disk (``cameraman512.p
   ``train_coded.py:50-65``, a binary random mask at 50% fill, and sub-pixel shifts
   normalised by the field side (``train_coded.py:68-70,159``);
 * measurements: Poisson counts of ``|model|^2 / scale`` stored as uint16, with one
-  global ``scale`` chosen so an average pattern holds the requested photon count.
+  global ``scale`` chosen so an average pattern holds the requested photon count; on the
+  device, ``synthesize_dataset`` (the reference's chunked forward,
+  ``train_ptychography.py:432-450``) and ``poisson_counts_device`` draw them without a
+  host round trip.
 """
 
 from __future__ import annotations
@@ -33,6 +37,8 @@ __all__ = [
     "angular_spectrum_transfer",
     "binary_mask",
     "coded_shifts",
+    "synthesize_dataset",
+    "poisson_counts_device",
 ]
 
 
@@ -170,3 +176,44 @@ def coded_shifts(count: int, max_px: float, n: int, rng: np.random.Generator | N
     rng = rng or np.random.default_rng(0)
     px = rng.uniform(-max_px, max_px, size=(count, 2))
     return (px / n).astype(np.float32)
+
+
+def synthesize_dataset(object_true, probe_true, positions, batch_size: int):
+    """Forward amplitudes of every scan position, ``batch_size`` positions per operator call.
+
+    The reference's ``synthesize_dataset`` (``train_ptychography.py:432-450``, under
+    ``torch.no_grad``): ``ptychoX_base`` over consecutive slices of ``positions``,
+    concatenated along the batch.  Tensors as for ``ptychoX_base``.
+    """
+    import torch
+
+    from .base import ptychoX_base
+
+    if batch_size <= 0:
+        raise ValueError("batch_size must be positive.")
+    with torch.no_grad():
+        chunks = [ptychoX_base(object_true, probe_true, positions[s:s + batch_size])
+                  for s in range(0, positions.shape[0], batch_size)]
+    return torch.cat(chunks, dim=0)
+
+
+def poisson_counts_device(amplitude, photons: float, seed: int = 0, per_pixel: bool = False,
+                          brightest: bool = False):
+    """Device twin of ``poisson_counts`` for amplitudes already on the GPU.
+
+    Returns uint16 Poisson counts of ``amplitude**2 / scale`` drawn with torch's device RNG
+    (seeded with ``seed``) and ``scale`` (a float32 value, used for the draw as well), with
+    ``scale`` chosen as in ``poisson_counts``.  Raises if any count exceeds uint16.
+    """
+    import torch
+
+    inten = amplitude.double() ** 2
+    sums = inten.flatten(1).sum(dim=1)
+    per_pattern = float(sums.max() if brightest else sums.mean())
+    denom = photons * (inten[0].numel() if per_pixel else 1)
+    scale = float(np.float32(per_pattern / denom))
+    gen = torch.Generator(device=amplitude.device).manual_seed(seed)
+    counts = torch.poisson(inten / scale, generator=gen)
+    if float(counts.max()) > 65535:
+        raise ValueError("Poisson counts saturate uint16; lower the photon count")
+    return counts.to(torch.int32).to(torch.uint16), scale

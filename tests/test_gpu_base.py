@@ -165,6 +165,29 @@ def test_chunked_workspace_matches():
     assert _abi.query("ptx_fft_supported", 7) == 0
 
 
+def test_synthesize_dataset_and_device_counts():
+    """``synth.synthesize_dataset`` (the reference's chunked forward) equals one operator call
+    over all positions bit for bit; device Poisson counts repeat for a seed and hold the
+    requested photons per pattern on average (5 standard deviations)."""
+    from ptychox_b200 import ptychoX_base, synth
+
+    rng = np.random.default_rng(21)
+    obj = cuda(synth.random_object(256, 256, rng))
+    probe = cuda(synth.gaussian_probe(64, 64, rng))
+    pos = cuda(synth.raster_positions(5, 40, 4, 2, rng))
+    amp = synth.synthesize_dataset(obj, probe, pos, batch_size=7)
+    assert torch.equal(amp, ptychoX_base(obj, probe, pos))
+    c1, s1 = synth.poisson_counts_device(amp, 1e4, seed=3)
+    c2, s2 = synth.poisson_counts_device(amp, 1e4, seed=3)
+    assert c1.dtype == torch.uint16 and torch.equal(c1, c2) and s1 == s2
+    total = float(c1.to(torch.float64).sum())
+    expect = float((amp.double() ** 2).sum()) / s1
+    assert abs(total - expect) < 5 * expect**0.5
+    assert abs(total / amp.shape[0] - 1e4) < 0.01 * 1e4
+    with pytest.raises(ValueError):
+        synth.synthesize_dataset(obj, probe, pos, batch_size=0)
+
+
 def test_errors_are_mapped():
     from ptychox_b200 import ptychoX_base
 
