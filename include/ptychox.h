@@ -282,6 +282,26 @@ int ptx_base_sweep_noalloc(const float* sample, int sample_h, int sample_w,
                            const uint16_t* measured, float scale,
                            double* loss, float* grad_sample, float* grad_probe, void* stream);
 
+/* ---- sub-pixel registration (positional tracking of coded / near-field scans) ---- */
+
+/* Workspace of ptx_reg_upsampled_peak (0 when usfac <= 2). */
+size_t ptx_reg_workspace_bytes(int batch, int rows, int cols, int usfac);
+
+/* The matrix-multiply DFT refinement of dftregistration (matlab/Examples/Near-field
+ * Ptychography/+misc/dftregistration.m:102-121 with dftups :150-185) for `batch` images:
+ * `cross_power` [batch][rows][cols] interleaved complex64 holds buf2ft .* conj(buf1ft);
+ * `row_center` / `col_center` (int32 [batch], device) the initial estimate times usfac
+ * (round(shift * usfac)).  The inverse DFT of each cross-power spectrum is evaluated on the
+ * n x n patch (n = ceil(1.5 usfac)) of the grid upsampled by usfac whose element
+ * (fix(n / 2), fix(n / 2)) sits at the estimate; `peak_rc` (int32 [batch][2]) receives the
+ * zero-based (row, col) of the first maximum of |CC| in column-major order (MATLAB's
+ * find(..., 1, 'first')) and `peak_cc` (interleaved complex128 [batch]) CC there,
+ * CC = conj(dftups); the upsampled DFT is summed in FP64.  The refined shift is
+ * estimate + (peak - fix(n / 2)) / usfac.  3 <= usfac <= 100000. */
+int ptx_reg_upsampled_peak(const float* cross_power, int batch, int rows, int cols, int usfac,
+                           const int* row_center, const int* col_center, int* peak_rc, double* peak_cc,
+                           void* workspace, size_t workspace_bytes, void* stream);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif
