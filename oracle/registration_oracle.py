@@ -12,7 +12,8 @@ It restates, in numpy (FP64), the MATLAB helpers of the reference's near-field e
   cross-correlation for the initial peak (``:90-101``), then a matrix-multiply DFT
   upsampled by ``usfac`` in a 1.5-pixel neighbourhood of it (``:102-121``), error and
   phase difference from the peak value (``:132-138``);
-* ``dftups`` (``:150-185``) and ``FTpad`` (``:189-224``), its two helpers;
+* ``dftups`` (``:150-185``) and ``FTpad`` (``:189-224``), its two helpers, and the
+  registered spectrum ``Greg`` (``:140-148``);
 * ``track_position.m:24-41`` and ``refine_position.m:25-55``: register every cropped
   measurement against a reference image (the first measurement, or the average of the
   measurements shifted back by their initial estimates) with a 20-pixel border removed.
@@ -32,7 +33,7 @@ from __future__ import annotations
 
 import numpy as np
 
-__all__ = ["dftregistration", "dftups", "ftpad", "track_position", "refine_position"]
+__all__ = ["dftregistration", "registered", "dftups", "ftpad", "track_position", "refine_position"]
 
 
 def _fix(x: float) -> int:
@@ -84,6 +85,17 @@ def dftups(x: np.ndarray, nor: int, noc: int, usfac: int, roff: float, coff: flo
     kernc = np.exp((-2j * np.pi / (nc * usfac)) * np.outer(fc, np.arange(noc) - coff))
     kernr = np.exp((-2j * np.pi / (nr * usfac)) * np.outer(np.arange(nor) - roff, fr))
     return kernr @ x @ kernc
+
+
+def registered(buf2ft: np.ndarray, output: np.ndarray, usfac: int) -> np.ndarray:
+    """``Greg`` (``dftregistration.m:140-148``): ``buf2ft`` shifted by the registration
+    output and multiplied by ``exp(i diffphase)``."""
+    nr, nc = buf2ft.shape
+    ncg, nrg = np.meshgrid(_freq(nc), _freq(nr))
+    g = np.asarray(buf2ft, dtype=np.complex128)
+    if usfac > 0:
+        g = g * np.exp(2j * np.pi * (-output[2] * nrg / nr - output[3] * ncg / nc))
+    return g * np.exp(1j * output[1])
 
 
 def dftregistration(buf1ft: np.ndarray, buf2ft: np.ndarray, usfac: int = 1) -> np.ndarray:

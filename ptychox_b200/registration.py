@@ -75,13 +75,15 @@ def _refine(q: torch.Tensor, usfac: int, rc: torch.Tensor, cc: torch.Tensor):
     return peak_rc.long(), peak_cc
 
 
-def dftregistration(buf1ft: torch.Tensor, buf2ft: torch.Tensor, usfac: int = 1) -> torch.Tensor:
+def dftregistration(buf1ft: torch.Tensor, buf2ft: torch.Tensor, usfac: int = 1, return_registered: bool = False):
     """``[error, diffphase, row_shift, col_shift]`` registering ``buf2ft`` to ``buf1ft``.
 
     ``buf1ft`` / ``buf2ft``: complex spectra (``fft2`` of the images) on the GPU, ``[h, w]``
     or ``[B, h, w]`` (a single spectrum on either side is broadcast).  ``usfac``: 0 (error
     and phase only), 1 (whole pixels), 2 (half pixels) or larger (1/usfac of a pixel).
-    Returns float64 ``[B, 4]``, or ``[4]`` when both inputs are 2-D.
+    Returns float64 ``[B, 4]``, or ``[4]`` when both inputs are 2-D; with
+    ``return_registered`` also ``Greg``, the spectrum of ``buf2ft`` shifted and phase-corrected
+    onto ``buf1ft`` (the second output of ``dftregistration.m:140-148``), complex64.
     """
     if buf1ft.ndim not in (2, 3) or buf2ft.ndim not in (2, 3):
         raise ValueError("buf1ft and buf2ft must be [h, w] or [batch, h, w] spectra.")
@@ -131,8 +133,17 @@ def dftregistration(buf1ft: torch.Tensor, buf2ft: torch.Tensor, usfac: int = 1) 
     rg00 = (b1.abs().double() ** 2).sum(dim=(-2, -1))
     rf00 = (b2.abs().double() ** 2).sum(dim=(-2, -1))
     error = torch.sqrt(torch.abs(1.0 - ccmax.abs() ** 2 / (rg00 * rf00)))
-    out = torch.stack([error, torch.angle(ccmax), row_shift, col_shift], dim=1)
-    return out[0] if single else out
+    diffphase = torch.angle(ccmax)
+    out = torch.stack([error, diffphase, row_shift, col_shift], dim=1)
+    if not return_registered:
+        return out[0] if single else out
+    fr = _freq(nr, dev).double()[None, :, None] / nr
+    fc = _freq(nc, dev).double()[None, None, :] / nc
+    phase = diffphase[:, None, None]
+    if usfac > 0:
+        phase = phase - 2 * math.pi * (row_shift[:, None, None] * fr + col_shift[:, None, None] * fc)
+    greg = b2 * torch.polar(torch.ones_like(phase), phase).to(torch.complex64)
+    return (out[0], greg[0]) if single else (out, greg)
 
 
 def _crop(stack: torch.Tensor, edge: int) -> torch.Tensor:
@@ -149,14 +160,18 @@ def _check_stack(im_raw_crop: torch.Tensor, edge: int) -> torch.Tensor:
     return im_raw_crop.to(torch.float32)
 
 
-def track_position(im_raw_crop: torch.Tensor, edge: int = 20, usfac: int = 600):
+def track_position(im_raw_crop: torch.Tensor, edge: int = 20, usfac: int = 600, return_registered: bool = False):
     """Initial positional tracking (``track_position.m:24-41``): every measurement of the
     ``[n, h, w]`` stack registered against the first, ``edge`` pixels of border removed.
-    Returns float64 ``(locX, locY)``."""
+    Returns float64 ``(locX, locY)``, and with ``return_registered`` also ``regi``, the
+    registered spectra of the cropped measurements (``[n, h - 2 edge, w - 2 edge]``)."""
     stack = _check_stack(im_raw_crop, edge)
     spectra = torch.fft.fft2(_crop(stack, edge).to(torch.complex64))
-    out = dftregistration(spectra[0], spectra, usfac)
-    return out[:, 3], out[:, 2]
+    res = dftregistration(spectra[0], spectra, usfac, return_registered=return_registered)
+    if return_registered:
+        out, regi = res
+        return out[:, 3], out[:, 2], regi
+    return res[:, 3], res[:, 2]
 
 
 def refine_position(im_raw_crop: torch.Tensor, loc_x0, loc_y0, edge: int = 20, usfac: int = 100):

@@ -69,6 +69,27 @@ def test_dftregistration_matches_oracle(usfac, shape):
     check_rows(one, want[2], usfac)
 
 
+@pytest.mark.parametrize("usfac", [0, 1, 100])
+def test_registered_spectrum_matches_oracle(usfac):
+    from ptychox_b200.registration import dftregistration, track_position
+
+    rng = np.random.default_rng(40 + usfac)
+    im = smooth_image(40, 56, rng)
+    stack = np.stack([shifted(im, dy, dx) for dy, dx in rng.uniform(-5, 5, size=(3, 2))])
+    b1, b2 = np.fft.fft2(im), np.fft.fft2(stack, axes=(-2, -1))
+    out, greg = dftregistration(torch.from_numpy(b1).cuda(), torch.from_numpy(b2).cuda(), usfac,
+                                return_registered=True)
+    for k in range(3):
+        # Greg from the GPU's own output, so only the FP32 spectrum and phase ramp differ
+        want = R.registered(b2[k], out[k].cpu().numpy(), usfac)
+        got = greg[k].cpu().numpy()
+        assert np.linalg.norm(got - want) / np.linalg.norm(want) < 1e-5
+    if usfac == 100:
+        big = np.stack([shifted(smooth_image(80, 80, rng, corr=0.3), 0, 0)] * 2)
+        lx, ly, regi = track_position(torch.from_numpy(big).cuda(), usfac=usfac, return_registered=True)
+        assert regi.shape == (2, 40, 40)
+
+
 def test_track_and_refine_match_oracle():
     from ptychox_b200.registration import refine_position, track_position
 
