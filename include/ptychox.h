@@ -70,8 +70,10 @@ int ptx_set_units_per_cta(int units);
  * call into a page-locked ring owned by the library (so `src` may be reused as soon as the
  * call returns) and a kernel reads them over the bus: a small per-step input such as a scan
  * is then neither queued on a copy engine behind another stream's large transfer nor
- * blocking the host as a pageable copy would.  Larger inputs take cudaMemcpyAsync.  No
- * reference counterpart: the reference moves scans with torch's `.to(device)`. */
+ * blocking the host as a pageable copy would.  Larger inputs, and calls on a stream that is
+ * being captured into a CUDA graph (whose copy node must re-read `src` on every replay),
+ * take cudaMemcpyAsync.  No reference counterpart: the reference moves scans with torch's
+ * `.to(device)`. */
 int ptx_stage_host_bytes(void* dst, const void* src, size_t bytes, void* stream);
 
 /* Optional per-kernel CUDA-event timing: when enabled every launch is bracketed by an

@@ -382,8 +382,17 @@ int ptx_stage_host_bytes(void* dst, const void* src, size_t bytes, void* stream)
   if (bytes == 0) return PTX_OK;
   if (!dst || !src) return ptx::set_error(PTX_ERR_INVALID_ARGUMENT, "null pointer argument");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // a stream being captured into a CUDA graph gets a copy node that re-reads `src` on every
+  // replay (a ring span would be filled once, at capture, and later reused)
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &capture) != cudaSuccess) {
+    cudaGetLastError();
+    capture = cudaStreamCaptureStatusActive;
+  }
   bool staged = false;
-  if (int st = ptx::stage_host(dst, src, bytes, s, &staged)) return st;
+  if (capture == cudaStreamCaptureStatusNone) {
+    if (int st = ptx::stage_host(dst, src, bytes, s, &staged)) return st;
+  }
   if (staged) return PTX_OK;
   return ptx::cuda_status(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, s), "ptx_stage_host_bytes copy");
 }

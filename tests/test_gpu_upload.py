@@ -101,6 +101,28 @@ def test_upload_small_paths():
     assert torch.equal(first.cpu(), pos) and torch.equal(second.cpu(), pos + 1)
 
 
+def test_capture_rereads_host_buffer_on_replay():
+    """Inside CUDA graph capture the staging is a copy node of the caller's page-locked
+    buffer, so every replay reads its current contents."""
+    from ptychox_b200._utils import upload_small
+
+    host = torch.arange(64, dtype=torch.int64).pin_memory()
+    dst = torch.zeros(64, dtype=torch.int64, device="cuda")
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        upload_small(host, dst.device, torch.long)  # warm-up outside the capture
+        with torch.cuda.graph(g, stream=s):
+            dst.copy_(upload_small(host, dst.device, torch.long))
+    torch.cuda.synchronize()
+    for k in (1, 5):
+        host.copy_(torch.arange(64, dtype=torch.int64) * k)
+        g.replay()
+        torch.cuda.synchronize()
+        assert torch.equal(dst.cpu(), torch.arange(64) * k)
+
+
 def test_pinned_scan_matches_device_scan():
     from ptychox_b200 import ptychoX_base_loss, synth
     from oracle import ptycho_oracle as O
@@ -118,7 +140,7 @@ def test_pinned_scan_matches_device_scan():
         p = torch.from_numpy(probe).cuda().requires_grad_(True)
         loss = ptychoX_base_loss(s, p, scan, meas_d, scale)
         loss.backward()
-        res.append((float(loss), s.grad.cpu(), p.grad.cpu()))
+        res.append((float(loss.detach()), s.grad.cpu(), p.grad.cpu()))
     # same inputs, same kernels; only the order of the gradient atomics differs between runs
     assert abs(res[0][0] - res[1][0]) <= 1e-12 * abs(res[1][0])
     for a, b in ((res[0][1], res[1][1]), (res[0][2], res[1][2])):
