@@ -299,7 +299,10 @@ __global__ void __launch_bounds__(ColPairCfg<N>::kThreads, ColPairCfg<N>::kThrea
     const int kr = t + S::T * m;
     const CPair F = UNIT_FULL ? v[m] : CPair{mul2(v[m].re, nrm), mul2(v[m].im, nrm)};
     const float2 s2 = fma2(F.re, F.re, mul2(F.im, F.im));
-    const float2 r = make_float2(rsqrt_nr(fmaxf(s2.x, 1e-37f)), rsqrt_nr(fmaxf(s2.y, 1e-37f)));
+    // rsqrt_nr on both lanes, its Newton-Raphson step in packed form (the same IEEE operations)
+    const float2 sc2 = make_float2(fmaxf(s2.x, 1e-37f), fmaxf(s2.y, 1e-37f));
+    const float2 y0 = make_float2(rsqrtf(sc2.x), rsqrtf(sc2.y));
+    const float2 r = mul2(y0, fma2(mul2(f2(-0.5f), sc2), mul2(y0, y0), f2(1.5f)));
     const float2 a = mul2(s2, r);
     const float2 inv =
         make_float2(a.x >= kEpsF32 ? r.x : 1.0f / kEpsF32, a.y >= kEpsF32 ? r.y : 1.0f / kEpsF32);
