@@ -37,8 +37,22 @@ __host__ __device__ __forceinline__ int plan_radix(const LinePlan& p, int s) {
 // --------------------------------------------------------------------------------------
 // complex helpers
 // --------------------------------------------------------------------------------------
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// complex add / subtract as one packed FP32x2 instruction on sm_100 (a - b as fma(b, -1, a),
+// which rounds once exactly like the subtraction)
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+  return __fadd2_rn(a, b);
+#else
+  return make_float2(a.x + b.x, a.y + b.y);
+#endif
+}
+__device__ __forceinline__ float2 csub(float2 a, float2 b) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+  return __ffma2_rn(b, make_float2(-1.f, -1.f), a);
+#else
+  return make_float2(a.x - b.x, a.y - b.y);
+#endif
+}
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
 }
