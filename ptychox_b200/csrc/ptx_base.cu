@@ -707,7 +707,7 @@ int check_common(const void* sample, int H, int W, const void* probe, int ph, in
     if constexpr (N > 0) {
       const int sm = RegLaunch<N>::col_smem();
       if (!st) st = ensure_smem((const void*)cols_sweep_pair<N, false, true>, ColPairCfg<N>::kSmemBytes);
-      if (!st) st = ensure_smem((const void*)cols_sweep_pair<N, false, true, true>, ColPairCfg<N>::kSmemBytes);
+      if (!st) st = ensure_smem((const void*)cols_sweep_pair<N, false, true, true, true>, ColPairCfg<N>::kSmemBytes);
       if (!st) st = ensure_smem((const void*)base_cols_reg<kColForward, N>, sm);
       if (!st) st = ensure_smem((const void*)base_cols_reg<kColBackward, N>, sm);
     } else {
@@ -788,7 +788,7 @@ void launch_cols(const BaseGeom& g, int frame0, int nframes, const uint16_t* mea
         // column DFT, amplitude-loss epilogue and inverse column DFT; counts fftshifted
         dim3 grid(num_tiles(g.pw), nframes);
         if (g.pw % kTile == 0) {
-          cols_sweep_pair<N, false, true, true><<<grid, ColPairCfg<N>::kThreads, ColPairCfg<N>::kSmemBytes, s>>>(
+          cols_sweep_pair<N, false, true, true, true><<<grid, ColPairCfg<N>::kThreads, ColPairCfg<N>::kSmemBytes, s>>>(
               g.scratch, g.pw, frame0, g.col.tw, measured, g.lut, 1.0f, grad_scale, inv_numel, loss);
         } else {
           cols_sweep_pair<N, false, true><<<grid, ColPairCfg<N>::kThreads, ColPairCfg<N>::kSmemBytes, s>>>(

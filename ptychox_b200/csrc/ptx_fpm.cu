@@ -400,6 +400,7 @@ int fpm_check(const void* object, int oh, int ow, const void* pupil, int lh, int
   dispatch_pow2(lh, [&](auto NT) {
     constexpr int N = decltype(NT)::value;
     if (!st) st = ensure_smem((const void*)cols_sweep_pair<N, true, false>, ColPairCfg<N>::kSmemBytes);
+    if (!st) st = ensure_smem((const void*)cols_sweep_pair<N, true, false, false, true>, ColPairCfg<N>::kSmemBytes);
     if (!st) st = ensure_smem((const void*)fpm_cols<kFpmForward, N>, ColPass<N>::kSmemBytes);
     if (!st) st = ensure_smem((const void*)fpm_cols<kFpmBackward, N>, ColPass<N>::kSmemBytes);
   });
@@ -454,8 +455,13 @@ void launch_cols(const FpmGeom& g, int frame0, int nf, const uint16_t* measured,
     if constexpr (MODE == kFpmSweep) {
       // inverse column DFT, 1/(h w), amplitude-loss epilogue, forward column DFT
       dim3 grid(num_tiles(g.lw), nf);
-      cols_sweep_pair<N, true, false><<<grid, ColPairCfg<N>::kThreads, ColPairCfg<N>::kSmemBytes, s>>>(
-          g.frames, g.lw, frame0, g.p_lh.tw, measured, g.lut, norm, grad_scale, inv_numel, loss);
+      if (g.lw % kTile == 0) {
+        cols_sweep_pair<N, true, false, false, true><<<grid, ColPairCfg<N>::kThreads, ColPairCfg<N>::kSmemBytes, s>>>(
+            g.frames, g.lw, frame0, g.p_lh.tw, measured, g.lut, norm, grad_scale, inv_numel, loss);
+      } else {
+        cols_sweep_pair<N, true, false><<<grid, ColPairCfg<N>::kThreads, ColPairCfg<N>::kSmemBytes, s>>>(
+            g.frames, g.lw, frame0, g.p_lh.tw, measured, g.lut, norm, grad_scale, inv_numel, loss);
+      }
       return;
     }
     dim3 grid(num_tiles(g.lw) * (kTile / kColsPerCta), nf);

@@ -228,9 +228,9 @@ struct ColPairCfg {
   static constexpr int kSmemBytes = kExchBytes + kTwBytes + kMeasBytes;
 };
 
-// UNIT_FULL: `norm` is 1 and `width` a multiple of the tile (every column pair exists), so the
-// epilogue drops the scaling and the per-column masks.
-template <int N, bool FIRST_INV, bool SHIFTED, bool UNIT_FULL = false>
+// UNIT_NORM: `norm` is 1 (the epilogue drops the scaling); FULL: `width` is a multiple of
+// the tile, so every column pair exists and the per-column masks go.
+template <int N, bool FIRST_INV, bool SHIFTED, bool UNIT_NORM = false, bool FULL = false>
 __global__ void __launch_bounds__(ColPairCfg<N>::kThreads, ColPairCfg<N>::kThreads <= 128 ? 2 : 1) cols_sweep_pair(
     float2* __restrict__ scratch, int width, int frame0, const float2* __restrict__ tw,
     const uint16_t* __restrict__ measured, const float* __restrict__ lut, float norm, float grad_scale,
@@ -246,8 +246,8 @@ __global__ void __launch_bounds__(ColPairCfg<N>::kThreads, ColPairCfg<N>::kThrea
   const int ct = blockIdx.x;
   const int f = blockIdx.y;
   const int c0 = ct * kTile;
-  const bool okA = UNIT_FULL || c0 + 2 * p < width;
-  const bool okB = UNIT_FULL || c0 + 2 * p + 1 < width;
+  const bool okA = FULL || c0 + 2 * p < width;
+  const bool okB = FULL || c0 + 2 * p + 1 < width;
   float2* tile = scratch + ((size_t)f * num_tiles(width) + ct) * N * kTile + 2 * p;
   const size_t g = (size_t)frame0 + f;
   float4* buf = sm4 + p * Cfg::LP4;
@@ -297,7 +297,7 @@ __global__ void __launch_bounds__(ColPairCfg<N>::kThreads, ColPairCfg<N>::kThrea
 #pragma unroll
   for (int m = 0; m < S::N1; ++m) {
     const int kr = t + S::T * m;
-    const CPair F = UNIT_FULL ? v[m] : CPair{mul2(v[m].re, nrm), mul2(v[m].im, nrm)};
+    const CPair F = UNIT_NORM ? v[m] : CPair{mul2(v[m].re, nrm), mul2(v[m].im, nrm)};
     const float2 s2 = fma2(F.re, F.re, mul2(F.im, F.im));
     // rsqrt_nr on both lanes, its Newton-Raphson step in packed form (the same IEEE operations)
     const float2 sc2 = make_float2(fmaxf(s2.x, 1e-37f), fmaxf(s2.y, 1e-37f));
