@@ -28,6 +28,8 @@ struct RegShape {
   static constexpr int C = N1 / T;                 // step-3 DFTs per thread (1 or 2)
   static constexpr int RP = T + 1;                 // exchange row pitch (odd)
   static constexpr int BUF = N1 * RP;              // exchange buffer per line (float2)
+  static constexpr int RPV = T + 2;                // even pitch of the row-pass exchange
+  static constexpr int BUFV = N1 * RPV;            // its buffer per line (float2)
   static_assert((1 << LOG) == N && N >= 4 && N <= 1024, "power of two in [4, 1024]");
 };
 
@@ -162,10 +164,11 @@ struct RegDft<32, INV> {
 
 // Line-buffer pitch (float2) for kernels whose threads run t-fastest (row passes): lines
 // sharing a half-warp land on disjoint bank sets.
+// Sized for the larger (even-pitch) exchange of the row passes.
 template <int N>
 __host__ __device__ constexpr int row_line_pitch() {
   using S = RegShape<N>;
-  return S::T >= 16 ? S::BUF : S::BUF + ((S::T - S::BUF % 16) + 16) % 16;
+  return S::T >= 16 ? S::BUFV : S::BUFV + ((S::T - S::BUFV % 16) + 16) % 16;
 }
 // Line-buffer pitch for kernels whose threads run column-fastest (column passes): a
 // half-warp holds 8 columns x 2 line threads, and with a pitch = 2 (mod 16) (in float2)
@@ -202,10 +205,16 @@ __device__ __forceinline__ void line_sync() {
 // every thread of the block (or warp) must call it.  TW_SHARED: `tw` points to a
 // shared-memory table laid out by thread, tw[k1 * T + t] = exp(-2 pi i t k1 / N) (see
 // load_twiddles_by_thread), so the T lanes of a line read consecutive words.
+//
+// The row-pass form (TW_SHARED, line buffers of row_line_pitch, 16-byte aligned) lays the
+// exchange out with the even pitch RPV, so step 3 reads its contiguous row two elements per
+// 16-byte load (half the shared-memory load instructions); with T lanes per line the loads
+// of a warp still take the minimum number of shared-memory wavefronts.
 template <int N, bool INV, bool BLOCK, bool TW_SHARED = false>
 __device__ __forceinline__ void reg_fft(float2 (&v)[RegShape<N>::N1], float2* buf, int t,
                                         const float2* __restrict__ tw) {
   using S = RegShape<N>;
+  constexpr int RP = TW_SHARED ? S::RPV : S::RP;
   RegDft<S::N1, INV>::run(v);
 #pragma unroll
   for (int k1 = 1; k1 < S::N1; ++k1) {
@@ -214,13 +223,23 @@ __device__ __forceinline__ void reg_fft(float2 (&v)[RegShape<N>::N1], float2* bu
     v[k1] = cmul(v[k1], w);
   }
 #pragma unroll
-  for (int k1 = 0; k1 < S::N1; ++k1) buf[k1 * S::RP + t] = v[k1];
+  for (int k1 = 0; k1 < S::N1; ++k1) buf[k1 * RP + t] = v[k1];
   line_sync<BLOCK>();
 #pragma unroll
   for (int q = 0; q < S::C; ++q) {
     float2 u[S::T];
+    if constexpr (TW_SHARED) {
+      const float4* row = reinterpret_cast<const float4*>(buf + (q * S::T + t) * RP);
 #pragma unroll
-    for (int j2 = 0; j2 < S::T; ++j2) u[j2] = buf[(q * S::T + t) * S::RP + j2];
+      for (int j = 0; j < S::T / 2; ++j) {
+        const float4 x = row[j];
+        u[2 * j] = make_float2(x.x, x.y);
+        u[2 * j + 1] = make_float2(x.z, x.w);
+      }
+    } else {
+#pragma unroll
+      for (int j2 = 0; j2 < S::T; ++j2) u[j2] = buf[(q * S::T + t) * RP + j2];
+    }
     RegDft<S::T, INV>::run(u);
 #pragma unroll
     for (int k2 = 0; k2 < S::T; ++k2) v[q + S::C * k2] = u[k2];
