@@ -284,6 +284,55 @@ int ptx_base_sweep_noalloc(const float* sample, int sample_h, int sample_w,
                            const uint16_t* measured, float scale,
                            double* loss, float* grad_sample, float* grad_probe, void* stream);
 
+/* ---- reconstruction server (continuous batching of whole reconstructions) ---------- */
+
+/* The reference drivers' training loop (python/train_ptychography.py:473-603, train_fpm.py,
+ * train_coded.py: per iteration a sweep, F.mse_loss and torch.optim.Adam with betas
+ * (0.9, 0.999), eps 1e-16) served natively for many problems at once.  Requests are copied
+ * at submit; a scheduler thread admits them first come first served while their resident
+ * bytes fit the HBM budget, keeps each admitted reconstruction on the device (one
+ * stream-ordered allocation), captures one iteration (fused sweep + one Adam step of each
+ * parameter) as a CUDA graph with the persistent passes bounded to 8 units per CTA, and
+ * replays the iterations of all active reconstructions concurrently on per-reconstruction
+ * streams (older ones at higher priority).  Python: ptychox_b200.native_server. */
+#define PTX_MODALITY_CONVENTIONAL 0
+#define PTX_MODALITY_FOURIER 1
+#define PTX_MODALITY_CODED 2
+#define PTX_MODALITY_NEARFIELD 3
+
+typedef struct ptx_recon_request {
+  int modality;            /* PTX_MODALITY_* */
+  int obj_h, obj_w;        /* object (conventional), object spectrum side (Fourier), field (coded) */
+  int aux_h, aux_w;        /* probe / pupil / coded surface or probe field (coded: = object) */
+  int batch;               /* positions, LEDs or shifts */
+  int downsample;          /* coded and near-field */
+  int iters;               /* iterations: one sweep and one Adam step of each parameter */
+  float scale;             /* observed amplitude = sqrt(scale * count) */
+  float lr_obj, lr_aux;    /* Adam learning rates */
+  int constrain_obj, constrain_aux;  /* PTX_CONSTRAIN_* projection after each step */
+  const float* obj0;       /* host, interleaved complex64 [obj_h][obj_w] */
+  const float* aux0;       /* host, complex64 [aux_h][aux_w] */
+  const void* scan;        /* host: int64 [batch][2] positions / LED corners, float32 [batch][2] shifts */
+  const uint16_t* measured;  /* host counts [batch][aux_h][aux_w], coded [batch][n/ds][n/ds] */
+  const float* transfer_1; /* host complex64 [n][n] (coded; NULL otherwise) */
+  const float* transfer_2; /* host complex64 [n][n] (coded and near-field) */
+} ptx_recon_request;
+
+/* Start a server on `device`; hbm_budget 0 = 70% of the free device memory. */
+int ptx_server_create(int device, size_t hbm_budget, int max_active, void** server);
+/* Queue a reconstruction (its arrays are copied at the call); *id identifies it.  A request
+ * whose resident bytes exceed the budget is refused with PTX_ERR_WORKSPACE, a conventional
+ * scan whose windows leave the object with PTX_ERR_OUT_OF_BOUNDS. */
+int ptx_server_submit(void* server, const ptx_recon_request* request, long long* id);
+/* Non-blocking.  *done = 1 when the reconstruction has finished: the final parameters are
+ * copied to object_out / aux_out (host, as obj0 / aux0; either may be NULL), the loss of its
+ * last sweep to *final_loss and submit-to-finish seconds to *latency_s, and the request is
+ * forgotten.  A failed request returns its error code (and is forgotten). */
+int ptx_server_poll(void* server, long long id, int* done, double* final_loss, double* latency_s,
+                    float* object_out, float* aux_out);
+/* Cancel queued requests, finish the active ones, stop the scheduler and free the server. */
+int ptx_server_destroy(void* server);
+
 /* ---- sub-pixel registration (positional tracking of coded / near-field scans) ---- */
 
 /* Workspace of ptx_reg_upsampled_peak (0 when usfac <= 2). */

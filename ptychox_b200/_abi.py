@@ -20,6 +20,11 @@ PTX_ERR_CUDA = 4
 PTX_ERR_OUT_OF_BOUNDS = 5
 PTX_ERR_TIMEOUT = 6
 
+PTX_MODALITY_CONVENTIONAL = 0
+PTX_MODALITY_FOURIER = 1
+PTX_MODALITY_CODED = 2
+PTX_MODALITY_NEARFIELD = 3
+
 PTX_CONSTRAIN_NONE = 0
 PTX_CONSTRAIN_UNIT_AMPLITUDE = 1
 PTX_CONSTRAIN_REAL_NONNEGATIVE = 2
@@ -64,6 +69,10 @@ SIGNATURES: dict[str, tuple] = {
     "ptx_base_sweep_noalloc": (_i, [_p, _i, _i, _p, _i, _i, _p, _i, _p, _f, _p, _p, _p, _p]),
     "ptx_reg_workspace_bytes": (_sz, [_i, _i, _i, _i]),
     "ptx_reg_upsampled_peak": (_i, [_p, _i, _i, _i, _i, _p, _p, _p, _p, _p, _sz, _p]),
+    "ptx_server_create": (_i, [_i, _sz, _i, _p]),
+    "ptx_server_submit": (_i, [_p, _p, _p]),
+    "ptx_server_poll": (_i, [_p, C.c_longlong, _p, _p, _p, _p, _p]),
+    "ptx_server_destroy": (_i, [_p]),
 }
 
 _lock = threading.Lock()

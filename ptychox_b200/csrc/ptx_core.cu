@@ -268,6 +268,8 @@ int persistent_grid(const void* kernel, int threads, int smem, long long units) 
   return static_cast<int>(std::max<long long>(1, std::min<long long>(grid, std::max<long long>(units, 1))));
 }
 
+int units_per_cta() { return g_units_per_cta.load(std::memory_order_relaxed); }
+
 // Device copy of page-locked host memory, read over the bus with loads that never hit a
 // stale cached line of system memory (ld.global.cv).  Grid-stride; 8-byte words when both
 // ends are 8-byte aligned, bytes otherwise.

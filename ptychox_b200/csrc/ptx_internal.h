@@ -53,6 +53,8 @@ int resident_ctas(const void* kernel, int threads, int smem);
 // Grid of a persistent pass over `units` work units: one wave of resident CTAs, or, when
 // ptx_set_units_per_cta(k > 0) is in force, enough CTAs that none takes more than k units.
 int persistent_grid(const void* kernel, int threads, int smem, long long units);
+// The bound set by ptx_set_units_per_cta (0: one wave, no bound).
+int units_per_cta();
 
 // Kernel kinds for the launch counter and the optional per-kernel event profiler.
 enum KernelId {

@@ -1,0 +1,69 @@
+"""The native reconstruction server (``ptx_server_*``) against the Python server.
+
+Both run the same iteration (fused sweep, one Adam step of each parameter) from the same
+requests, so their results agree to the serving tolerance: relative L2 1e-4 on the final
+object and probe / pupil / mask and 1e-4 on the final loss (float atomics add in a varying
+order and 12 Adam iterations carry the differences forward).
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_l2
+from test_gpu_serving import small_mix
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _lib():
+    from ptychox_b200 import _abi
+
+    _abi.load()
+    assert torch.cuda.is_available()
+
+
+def test_native_matches_python_server():
+    from ptychox_b200.native_server import NativeReconstructionServer
+    from ptychox_b200.serving import ReconstructionServer
+
+    reqs = small_mix()
+    want = ReconstructionServer("cuda", max_active=8).run(reqs, realtime=False)
+    with NativeReconstructionServer(0, max_active=8) as srv:
+        got = srv.run(reqs)
+    for g, w in zip(got, want):
+        assert g.rid == w.rid and g.modality == w.modality
+        assert np.isfinite(g.final_loss) and g.finished >= g.arrival
+        assert abs(g.final_loss - w.final_loss) <= 1e-4 * abs(w.final_loss)
+        assert rel_l2(g.obj, w.obj) < 1e-4
+        assert rel_l2(g.aux, w.aux) < 1e-4
+
+
+def test_native_one_at_a_time_budget_and_errors():
+    from ptychox_b200 import _abi
+    from ptychox_b200.native_server import NativeReconstructionServer
+    from ptychox_b200.serving import ReconstructionServer
+
+    reqs = small_mix()[:3]
+    want = ReconstructionServer("cuda").run(reqs, realtime=False)
+    # a budget of one reconstruction's resident bytes still serves them all, one after another
+    with NativeReconstructionServer(0, hbm_budget=1 << 20, max_active=8) as small:
+        with pytest.raises(_abi.PtychoXError):
+            small.submit(reqs[0])  # more than the budget
+    with NativeReconstructionServer(0, hbm_budget=600 << 20, max_active=1) as srv:
+        got = srv.run(reqs)
+        for g, w in zip(got, want):
+            assert abs(g.final_loss - w.final_loss) <= 1e-4 * abs(w.final_loss)
+            assert rel_l2(g.obj, w.obj) < 1e-4
+        with pytest.raises(ValueError):
+            srv.poll(12345)
+        bad = small_mix()[0]
+        bad.pos = bad.pos + 10_000  # windows outside the object are refused at submit
+        with pytest.raises(ValueError):
+            srv.submit(bad)
+        bad2 = small_mix()[1]
+        bad2.modality = "conventional"
+        bad2.iters = 0
+        with pytest.raises(ValueError):
+            srv.submit(bad2)
