@@ -728,6 +728,31 @@ def run_reference(args) -> None:
 # ---------------------------------------------------------------------------------------
 
 
+def run_native(reqs, warm, dev, max_active):
+    """The stream through the native server: each request submitted at its arrival time,
+    all polled until finished; returns (results in rid order, wall seconds to the last)."""
+    from ptychox_b200.native_server import NativeReconstructionServer
+
+    with NativeReconstructionServer(dev.index or 0, max_active=max_active) as srv:
+        srv.run(warm)
+        pending = sorted(reqs, key=lambda r: (r.arrival, r.rid))
+        ids, out = {}, {}
+        t0 = time.perf_counter()
+        while pending or ids:
+            now = time.perf_counter() - t0
+            while pending and pending[0].arrival <= now:
+                r = pending.pop(0)
+                ids[srv.submit(r)] = r.rid
+            for sid in list(ids):
+                res = srv.poll(sid)
+                if res is not None:
+                    out[ids.pop(sid)] = res
+            if ids or pending:
+                time.sleep(5e-4)
+        wall = time.perf_counter() - t0
+    return [out[k] for k in sorted(out)], wall
+
+
 def run_serving(args) -> None:
     """Served mixed stream vs one-at-a-time plain solves on the same GPU.
 
@@ -769,6 +794,7 @@ def run_serving(args) -> None:
     t0 = time.perf_counter()
     plain = run_plain(reqs, dev, realtime=True)
     t_plain = time.perf_counter() - t0
+    native, t_native = run_native(reqs, warm, dev, args.max_active)
 
     sweeps = sum(r.sweeps for r in served)
     lat_s = [r.latency for r in served]
@@ -799,6 +825,13 @@ def run_serving(args) -> None:
         "plain": {"wall_s": t_plain, "sweeps_per_s": sweeps / t_plain, "p50_latency_s": percentile(lat_p, 50),
                   "p99_latency_s": percentile(lat_p, 99),
                   "method": "one request at a time: unfused operators + F.mse_loss + torch.optim.Adam"},
+        "native": {"wall_s": t_native, "sweeps_per_s": sweeps / t_native,
+                   "p50_latency_s": percentile([r.latency for r in native], 50),
+                   "p99_latency_s": percentile([r.latency for r in native], 99),
+                   "final_loss_rel_diff_max_vs_served": max(abs(a.final_loss - b.final_loss) / abs(b.final_loss)
+                                                          for a, b in zip(native, served)),
+                   "method": "the same service in libptychox's scheduler thread (C ABI ptx_server_*), "
+                             "requests submitted at their arrival times and polled"},
         "throughput_ratio_served_over_plain": t_plain / t_served,
         "final_loss_rel_diff_max": max(rel_final),
         "gpu_launches": launches,

@@ -6,7 +6,8 @@
 // probe / pupil / coded surface, scan, counts, schedule); the server copies it at submit,
 // admits requests first come first served while their resident bytes fit the HBM budget,
 // and keeps each admitted reconstruction's state on the device: parameters, gradients,
-// Adam moments, counts, scan and workspace in one stream-ordered allocation.  One iteration
+// Adam moments, counts, scan and workspace in one allocation from the server's own
+// stream-ordered pool (kept mapped between reconstructions).  One iteration
 // (fused sweep + one Adam step of each parameter) is captured once per reconstruction as a
 // CUDA graph, with the persistent passes bounded to 8 units per CTA at capture so the
 // kernels of concurrent reconstructions interleave CTA by CTA; a scheduler thread replays
@@ -73,6 +74,9 @@ struct Server {
   int device = 0;
   size_t budget = 0;
   int max_active = 8;
+  // the server's own stream-ordered pool: memory freed by a finished reconstruction stays
+  // mapped for the next one instead of returning to the system at every synchronisation
+  cudaMemPool_t pool = nullptr;
   std::mutex mu;
   std::condition_variable cv;
   std::deque<Request*> queued;
@@ -164,7 +168,7 @@ void release(Slot& s) {
 }
 
 // Allocate, upload, warm up and capture one reconstruction; PTX_OK or an error code.
-int admit(Slot& s, Request* r, int priority) {
+int admit(Slot& s, Request* r, int priority, cudaMemPool_t pool) {
   s.req = r;
   const ptx_recon_request& d = r->d;
   if (cudaStreamCreateWithPriority(&s.stream, cudaStreamNonBlocking, priority) != cudaSuccess) {
@@ -172,7 +176,9 @@ int admit(Slot& s, Request* r, int priority) {
   }
   const size_t po = align256(obj_elems(d) * sizeof(float2)), pa = align256(aux_elems(d) * sizeof(float2));
   const size_t total = slot_bytes(*r);
-  if (cudaMallocAsync(&s.base, total, s.stream) != cudaSuccess) return cuda_status(cudaGetLastError(), "server alloc");
+  if (cudaMallocFromPoolAsync(&s.base, total, pool, s.stream) != cudaSuccess) {
+    return cuda_status(cudaGetLastError(), "server alloc");
+  }
   char* p = static_cast<char*>(s.base);
   auto take = [&](size_t n) {
     char* q = p;
@@ -293,7 +299,7 @@ void serve(Server* sv) {
       }
       Slot s;
       const int prio = std::max(greatest, std::min(least, greatest + (int)active.size()));
-      const int e = admit(s, r, prio);
+      const int e = admit(s, r, prio, sv->pool);
       if (e) {
         release(s);
         std::lock_guard<std::mutex> lock(sv->mu);
@@ -407,6 +413,16 @@ int ptx_server_create(int device, size_t hbm_budget, int max_active, void** serv
     hbm_budget = free_b / 10 * 7;
   }
   sv->budget = hbm_budget;
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  if (cudaMemPoolCreate(&sv->pool, &props) != cudaSuccess) {
+    delete sv;
+    return cuda_status(cudaGetLastError(), "server memory pool");
+  }
+  unsigned long long keep = ~0ull;
+  cudaMemPoolSetAttribute(sv->pool, cudaMemPoolAttrReleaseThreshold, &keep);
   sv->worker = std::thread(serve, sv);
   *server = sv;
   return PTX_OK;
@@ -494,6 +510,7 @@ int ptx_server_destroy(void* server) {
   }
   sv->cv.notify_all();
   if (sv->worker.joinable()) sv->worker.join();
+  if (sv->pool) cudaMemPoolDestroy(sv->pool);
   delete sv;
   return PTX_OK;
 }
