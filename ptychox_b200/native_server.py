@@ -17,7 +17,7 @@ from . import _abi
 from .optim import CONSTRAINTS
 from .serving import ReconRequest, ReconResult
 
-__all__ = ["PtxReconRequest", "NativeReconstructionServer"]
+__all__ = ["PtxReconRequest", "NativeReconstructionServer", "ReplicaServer"]
 
 _MODALITY = {
     "conventional": _abi.PTX_MODALITY_CONVENTIONAL,
@@ -123,3 +123,63 @@ class NativeReconstructionServer:
             self.close()
         except Exception:
             pass
+
+
+class ReplicaServer:
+    """Serving replicas: one native server per device in ``devices`` (a device may repeat),
+    each request pinned to the replica with the fewest outstanding requests; no
+    communication between replicas (the multi-GPU mode of the reconstruction service)."""
+
+    def __init__(self, devices, hbm_budget: int = 0, max_active: int = 8):
+        self.replicas = [NativeReconstructionServer(int(d), hbm_budget, max_active) for d in devices]
+        self._where: dict[int, tuple[int, int]] = {}  # our id -> (replica, its id)
+        self._outstanding = [0] * len(self.replicas)
+        self._next = 1
+
+    def submit(self, req: ReconRequest) -> int:
+        k = min(range(len(self.replicas)), key=lambda i: (self._outstanding[i], i))
+        sid = self.replicas[k].submit(req)
+        rid = self._next
+        self._next += 1
+        self._where[rid] = (k, sid)
+        self._outstanding[k] += 1
+        return rid
+
+    def replica_of(self, rid: int) -> int:
+        return self._where[rid][0]
+
+    def poll(self, rid: int) -> ReconResult | None:
+        k, sid = self._where[rid]
+        try:
+            res = self.replicas[k].poll(sid)
+        except Exception:
+            del self._where[rid]
+            self._outstanding[k] -= 1
+            raise
+        if res is not None:
+            del self._where[rid]
+            self._outstanding[k] -= 1
+        return res
+
+    def run(self, requests: list[ReconRequest], poll_interval: float = 1e-3) -> list[ReconResult]:
+        """Submit all ``requests`` now and wait for them; results in ``rid`` order."""
+        ids = {self.submit(r): r.rid for r in requests}
+        out = {}
+        while ids:
+            for sid in list(ids):
+                res = self.poll(sid)
+                if res is not None:
+                    out[ids.pop(sid)] = res
+            if ids:
+                time.sleep(poll_interval)
+        return [out[k] for k in sorted(out)]
+
+    def close(self) -> None:
+        for r in self.replicas:
+            r.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -67,3 +67,28 @@ def test_native_one_at_a_time_budget_and_errors():
         bad2.iters = 0
         with pytest.raises(ValueError):
             srv.submit(bad2)
+
+
+def test_replicas_spread_requests_and_match():
+    """Two replicas (here both on device 0) take requests in turn and return what one
+    native server returns."""
+    from ptychox_b200.native_server import NativeReconstructionServer, ReplicaServer
+
+    reqs = small_mix()
+    with NativeReconstructionServer(0) as one:
+        want = one.run(reqs)
+    with ReplicaServer([0, 0]) as pool:
+        ids = [pool.submit(r) for r in reqs]
+        assert {pool.replica_of(i) for i in ids} == {0, 1}
+        got = {}
+        while len(got) < len(ids):
+            for i in ids:
+                if i not in got:
+                    res = pool.poll(i)
+                    if res is not None:
+                        got[i] = res
+    for i, w in zip(ids, want):
+        g = got[i]
+        assert g.rid == w.rid
+        assert abs(g.final_loss - w.final_loss) <= 1e-4 * abs(w.final_loss)
+        assert rel_l2(g.obj, w.obj) < 1e-4
