@@ -294,7 +294,10 @@ int ptx_base_sweep_noalloc(const float* sample, int sample_h, int sample_w,
  * stream-ordered allocation), captures one iteration (fused sweep + one Adam step of each
  * parameter) as a CUDA graph with the persistent passes bounded to 8 units per CTA, and
  * replays the iterations of all active reconstructions concurrently on per-reconstruction
- * streams (older ones at higher priority).  Python: ptychox_b200.native_server. */
+ * streams (older ones at higher priority).  While the scheduler captures a reconstruction
+ * the process-wide ptx_set_units_per_cta bound is 8 (restored after the capture), so sweeps
+ * that other host threads launch at that moment also take bounded units.  Python:
+ * ptychox_b200.native_server. */
 #define PTX_MODALITY_CONVENTIONAL 0
 #define PTX_MODALITY_FOURIER 1
 #define PTX_MODALITY_CODED 2

@@ -315,7 +315,10 @@ void serve(Server* sv) {
     for (Slot& s : active) {
       int err = 0;
       progressed |= launch_next(s, &err);
-      if (err) s.req->status = -err;
+      if (err) {
+        std::lock_guard<std::mutex> lock(sv->mu);
+        s.req->status = -err;
+      }
     }
     // retire finished (or failed) reconstructions
     for (size_t i = 0; i < active.size();) {
