@@ -136,6 +136,19 @@ int ptx_base_sweep(const float* sample, int sample_h, int sample_w,
                    double* loss, float* grad_sample, float* grad_probe,
                    void* workspace, size_t workspace_bytes, void* stream);
 
+/* ptx_base_sweep for square 32-, 64- or 128-point probes (PTX_ERR_UNSUPPORTED_SIZE
+ * otherwise), same arguments and results: one CTA runs the whole sweep of a frame in shared
+ * memory (gather, row and column DFTs with the loss epilogue, inverse DFTs, gradient
+ * scatter), so a sweep is the prologue and one launch, with no scratch frames in HBM (the
+ * workspace still holds the count-decode table and the error word).  The Python operators
+ * use it for such probes. */
+int ptx_base_sweep_small(const float* sample, int sample_h, int sample_w,
+                         const float* probe, int probe_h, int probe_w,
+                         const int64_t* positions_xy, int batch,
+                         const uint16_t* measured, float scale,
+                         double* loss, float* grad_sample, float* grad_probe,
+                         void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---- Fourier ptychography --------------------------------------------------------
  * Operator  A[b] = |ifft2(fftshift(S[window_b] * pupil))|, S = fft2(object), window_b the
  * (lh x lw) block at rows (ly+r+H/2) % H, columns (lx+c+W/2) % W of S.

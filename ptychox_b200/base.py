@@ -103,6 +103,9 @@ class PtychoXBaseFunction(torch.autograd.Function):
         return grad_sample, grad_probe, None, None
 
 
+SMALL_FRAMES = (32, 64, 128)
+
+
 def base_sweep(sample, probe, positions, measured, scale, ws=None):
     """Run one fused sweep on validated device tensors; returns ``(loss, grad_sample, grad_probe)``.
 
@@ -117,8 +120,10 @@ def base_sweep(sample, probe, positions, measured, scale, ws=None):
     gp = torch.empty_like(probe)
     if ws is None:
         ws = workspace(_abi.query("ptx_base_workspace_bytes", ph, pw, batch), dev)
+    # square 32 / 64 / 128 probes: the one-CTA-per-frame sweep (frame resident in shared memory)
+    entry = "ptx_base_sweep_small" if ph == pw and pw in SMALL_FRAMES else "ptx_base_sweep"
     with torch.cuda.device(dev):
-        _abi.call("ptx_base_sweep", ptr(sample), sample.shape[0], sample.shape[1], ptr(probe), ph, pw,
+        _abi.call(entry, ptr(sample), sample.shape[0], sample.shape[1], ptr(probe), ph, pw,
                   ptr(positions), batch, ptr(measured), float(scale), ptr(loss), ptr(gs), ptr(gp), ptr(ws),
                   ws.numel(), stream_handle(dev))
     return loss, gs, gp

@@ -633,6 +633,108 @@ __global__ void __launch_bounds__(128, 2) base_rows_adjoint_reg(
   }
 }
 
+// ---------------------------------------------------------------------------------------
+// Small frames (square power-of-two probes up to 128): the whole sweep of a frame in one
+// CTA.  A 128 x 128 complex frame is 128 KB, so it stays in shared memory from the gather
+// to the gradient scatter: gather O x P, row DFTs, column DFTs with the loss epilogue and the
+// inverse column DFTs, inverse row DFTs and the scatter of G conj(P) into grad_O and
+// G conj(O) into grad_P (float2 atomics), with no scratch frames in HBM and one launch per
+// sweep.  CTAs are persistent over frames (frame f = blockIdx.x + k gridDim.x).  The same
+// arithmetic as the three-pass sweep: register DFTs of the rows and columns, the amplitude
+// epilogue on fftshifted counts decoded through the table.
+template <int N>
+struct FrameCfg {
+  static constexpr int kThreads = 256;
+  static constexpr int T = RegShape<N>::T;
+  static constexpr int kLines = kThreads / T;          // lines transformed at once
+  static constexpr int FP = N + 4;                     // frame row pitch (float2): conflict-free columns
+  static constexpr int LP = row_line_pitch<N>();       // exchange buffer per line
+  static constexpr int kFrameF2 = N * FP;
+  static constexpr int kSmemBytes = (kFrameF2 + kLines * LP) * (int)sizeof(float2);
+};
+
+template <int N>
+__global__ void __launch_bounds__(256, 1) base_sweep_frame(
+    const float2* __restrict__ sample, int H, int W, const float2* __restrict__ probe,
+    const int64_t* __restrict__ pos, int nframes, const uint16_t* __restrict__ measured,
+    const float* __restrict__ lut, float grad_scale, double inv_numel, double* __restrict__ loss,
+    float2* __restrict__ grad_sample, float2* __restrict__ grad_probe, const float2* __restrict__ tw,
+    unsigned* __restrict__ err) {
+  using S = RegShape<N>;
+  using Cfg = FrameCfg<N>;
+  extern __shared__ float2 sm[];
+  float2* F = sm;                                       // [N][FP]
+  const int tid = threadIdx.x;
+  const int l = tid / S::T, t = tid - l * S::T;
+  float2* buf = sm + Cfg::kFrameF2 + l * Cfg::LP;
+  double part = 0.0;
+  for (int f = blockIdx.x; f < nframes; f += gridDim.x) {
+    const long long x0 = pos[2 * f], y0 = pos[2 * f + 1];
+    if (!window_ok(x0, y0, N, N, H, W)) {
+      if (tid == 0) atomicOr(err, 1u);
+      continue;  // uniform across the CTA
+    }
+    const float2* win = sample + y0 * W + x0;
+    // gather O x P
+    for (int i = tid; i < N * N; i += Cfg::kThreads) {
+      const int r = i / N, c = i - r * N;
+      F[r * Cfg::FP + c] = cmul(win[(size_t)r * W + c], __ldg(&probe[i]));
+    }
+    __syncthreads();
+    // forward row DFTs
+    for (int r = l; r < N; r += Cfg::kLines) {
+      float2 v[S::N1];
+#pragma unroll
+      for (int j = 0; j < S::N1; ++j) v[j] = F[r * Cfg::FP + t + S::T * j];
+      reg_fft<N, false, false>(v, buf, t, tw);
+#pragma unroll
+      for (int m = 0; m < S::N1; ++m) F[r * Cfg::FP + t + S::T * m] = v[m];
+    }
+    __syncthreads();
+    // column DFTs, amplitude-loss epilogue against the fftshifted counts, inverse column DFTs
+    const uint16_t* cnt = measured + (size_t)f * N * N;
+    for (int c = l; c < N; c += Cfg::kLines) {
+      float2 v[S::N1];
+#pragma unroll
+      for (int j = 0; j < S::N1; ++j) v[j] = F[(t + S::T * j) * Cfg::FP + c];
+      reg_fft<N, false, false>(v, buf, t, tw);
+      const int ic = (c + N / 2) & (N - 1);
+#pragma unroll
+      for (int m = 0; m < S::N1; ++m) {
+        const int kr = t + S::T * m;
+        const int ir = (kr + N / 2) & (N - 1);
+        const float y = __ldg(&lut[cnt[ir * N + ic]]);
+        float a, inv;
+        abs_and_inv(v[m], kEps, a, inv);
+        const float rr = a - y;
+        part += static_cast<double>(rr * rr);
+        v[m] = cscale(v[m], grad_scale * rr * inv);
+      }
+      reg_fft<N, true, false>(v, buf, t, tw);
+#pragma unroll
+      for (int j = 0; j < S::N1; ++j) F[(t + S::T * j) * Cfg::FP + c] = v[j];
+    }
+    __syncthreads();
+    // inverse row DFTs and the gradient scatter
+    float2* gwin = grad_sample + y0 * W + x0;
+    for (int r = l; r < N; r += Cfg::kLines) {
+      float2 v[S::N1];
+#pragma unroll
+      for (int j = 0; j < S::N1; ++j) v[j] = F[r * Cfg::FP + t + S::T * j];
+      reg_fft<N, true, false>(v, buf, t, tw);
+#pragma unroll
+      for (int m = 0; m < S::N1; ++m) {
+        const int c = t + S::T * m;
+        const float2 G = v[m];
+        atomicAdd(&gwin[(size_t)r * W + c], cmulc(G, __ldg(&probe[r * N + c])));
+        atomicAdd(&grad_probe[r * N + c], cmulc(G, win[(size_t)r * W + c]));
+      }
+    }
+    __syncthreads();
+  }
+  block_add_double(part, inv_numel, loss);
+}
+
 template <int N>
 struct RegLaunch {
   static constexpr int T = RegShape<N>::T;
@@ -911,6 +1013,57 @@ int ptx_base_sweep(const float* sample, int sample_h, int sample_w, const float*
     launch_rows_adjoint(g, S, P, pos, nf, GS, GP, s);
   }
   return cuda_status(cudaGetLastError(), "ptx_base_sweep launch");
+}
+
+int ptx_base_sweep_small(const float* sample, int sample_h, int sample_w, const float* probe, int probe_h,
+                         int probe_w, const int64_t* positions_xy, int batch, const uint16_t* measured, float scale,
+                         double* loss, float* grad_sample, float* grad_probe, void* workspace, size_t workspace_bytes,
+                         void* stream) {
+  if (!(probe_h == probe_w && (probe_w == 32 || probe_w == 64 || probe_w == 128))) {
+    return set_error(PTX_ERR_UNSUPPORTED_SIZE, "ptx_base_sweep_small takes square 32, 64 or 128 probes (got %d x %d)",
+                     probe_h, probe_w);
+  }
+  BaseGeom g;
+  if (int st = check_common(sample, sample_h, sample_w, probe, probe_h, probe_w, positions_xy, batch, workspace,
+                            workspace_bytes, &g)) {
+    return st;
+  }
+  if ((!measured && batch > 0) || !loss || !grad_sample || !grad_probe) {
+    return set_error(PTX_ERR_INVALID_ARGUMENT, "null pointer argument");
+  }
+  if (!(scale > 0.f)) return set_error(PTX_ERR_INVALID_ARGUMENT, "scale must be positive");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  float2* GS = reinterpret_cast<float2*>(grad_sample);
+  float2* GP = reinterpret_cast<float2*>(grad_probe);
+  const double numel = (double)batch * probe_h * probe_w;
+  const float grad_scale = static_cast<float>(2.0 / std::max(numel, 1.0));
+  {
+    const size_t ns = (size_t)sample_h * sample_w, np = (size_t)probe_h * probe_w;
+    prof_begin(kMiscKernel, s);
+    sweep_prologue_kernel<<<prologue_blocks(ns, sm_count()), 256, 0, s>>>(GS, ns, GP, np, loss, g.err, g.lut, scale);
+    prof_end(kMiscKernel, s);
+  }
+  if (batch == 0) return cuda_status(cudaGetLastError(), "ptx_base_sweep_small launch");
+  const float2* S = reinterpret_cast<const float2*>(sample);
+  const float2* P = reinterpret_cast<const float2*>(probe);
+  int st = PTX_OK;
+  dispatch_len(probe_w, [&](auto NT) {
+    constexpr int N = decltype(NT)::value;
+    if constexpr (N == 32 || N == 64 || N == 128) {
+      using Cfg = FrameCfg<N>;
+      st = ensure_smem((const void*)base_sweep_frame<N>, Cfg::kSmemBytes);
+      if (st) return;
+      const int grid = persistent_grid((const void*)base_sweep_frame<N>, Cfg::kThreads, Cfg::kSmemBytes, batch);
+      prof_begin(kBaseRowsForward, s);
+      base_sweep_frame<N><<<grid, Cfg::kThreads, Cfg::kSmemBytes, s>>>(S, sample_h, sample_w, P, positions_xy, batch,
+                                                                       measured, g.lut, grad_scale,
+                                                                       1.0 / std::max(numel, 1.0), loss, GS, GP,
+                                                                       g.row.tw, g.err);
+      prof_end(kBaseRowsForward, s);
+    }
+  });
+  if (st) return st;
+  return cuda_status(cudaGetLastError(), "ptx_base_sweep_small launch");
 }
 
 }  // extern "C"
