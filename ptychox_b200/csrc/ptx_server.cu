@@ -127,8 +127,10 @@ size_t slot_bytes(const Request& r) {
 int run_sweep(const Slot& s) {
   const ptx_recon_request& d = s.req->d;
   if (d.modality == PTX_MODALITY_CONVENTIONAL) {
-    return ptx_base_sweep(s.obj, d.obj_h, d.obj_w, s.aux, d.aux_h, d.aux_w, static_cast<const int64_t*>(s.scan),
-                          d.batch, s.meas, d.scale, s.loss, s.g_obj, s.g_aux, s.ws, s.req->ws_bytes, s.stream);
+    const bool small = d.aux_h == d.aux_w && (d.aux_w == 32 || d.aux_w == 64 || d.aux_w == 128);
+    return (small ? ptx_base_sweep_small : ptx_base_sweep)(
+        s.obj, d.obj_h, d.obj_w, s.aux, d.aux_h, d.aux_w, static_cast<const int64_t*>(s.scan), d.batch, s.meas,
+        d.scale, s.loss, s.g_obj, s.g_aux, s.ws, s.req->ws_bytes, s.stream);
   }
   if (d.modality == PTX_MODALITY_FOURIER) {
     return ptx_fpm_sweep(s.obj, d.obj_h, d.obj_w, s.aux, d.aux_h, d.aux_w, static_cast<const int64_t*>(s.scan),

@@ -161,7 +161,8 @@ class _Slot:
         s = self.stream_handle
         if r.modality == "conventional":
             (h, w), (ph, pw) = self.obj.shape, self.aux.shape
-            _abi.call("ptx_base_sweep", ptr(self.obj), h, w, ptr(self.aux), ph, pw, ptr(self.pos), r.units(),
+            entry = "ptx_base_sweep_small" if ph == pw and pw in (32, 64, 128) else "ptx_base_sweep"
+            _abi.call(entry, ptr(self.obj), h, w, ptr(self.aux), ph, pw, ptr(self.pos), r.units(),
                       ptr(self.meas), float(r.scale), ptr(self.loss), ptr(self.g_obj), ptr(self.g_aux), ptr(self.ws),
                       self.ws.numel(), s)
         elif r.modality == "fourier":
