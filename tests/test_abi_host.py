@@ -58,6 +58,33 @@ def test_pure_host_entry_points(lib):
     assert lib.ptx_set_units_per_cta(0) == 0
 
 
+def test_new_entry_points_refuse_bad_arguments_on_the_host(lib):
+    """Checks that run before any CUDA call: the small-frame sweep's size rule, the server's
+    device and argument checks, the registration workspace query."""
+    import ctypes as C
+
+    from ptychox_b200 import _abi
+
+    # ptx_base_sweep_small takes square 32 / 64 / 128 probes only
+    assert lib.ptx_base_sweep_small(None, 256, 256, None, 64, 32, None, 1, None, 1.0, None, None, None, None, 0,
+                                    None) == _abi.PTX_ERR_UNSUPPORTED_SIZE
+    assert "square 32, 64 or 128" in _abi.last_error()
+    # the server needs a CUDA device and positive slot counts
+    h = C.c_void_p()
+    assert lib.ptx_server_create(0, 0, 0, C.addressof(h)) == _abi.PTX_ERR_INVALID_ARGUMENT
+    assert lib.ptx_server_create(-1, 0, 8, C.addressof(h)) == _abi.PTX_ERR_INVALID_ARGUMENT
+    if not torch.cuda.is_available():
+        assert lib.ptx_server_create(0, 0, 8, C.addressof(h)) == _abi.PTX_ERR_INVALID_ARGUMENT
+    assert not h.value
+    assert lib.ptx_server_create(0, 0, 8, None) == _abi.PTX_ERR_INVALID_ARGUMENT
+    assert lib.ptx_server_destroy(None) == _abi.PTX_OK
+    # registration workspace: none up to usfac 2, else FP64 patches of ceil(1.5 usfac)^2 and
+    # n_out x rows per image
+    assert lib.ptx_reg_workspace_bytes(3, 64, 64, 2) == 0
+    assert lib.ptx_reg_workspace_bytes(2, 64, 80, 600) == 16 * 2 * 900 * (64 + 900)
+    assert lib.ptx_stage_host_bytes(None, None, 0, None) == _abi.PTX_OK  # nothing to copy
+
+
 def test_reference_input_checks_and_messages():
     from ptychox_b200._utils import check_complex_scan_inputs
 
