@@ -11,8 +11,11 @@ Our arm prints one JSON line (rank 0) with ``value`` = sweeps/s over all ranks f
 device-resident inputs (CUDA events per step, L2 flushed between steps, max over
 ranks), ``e2e`` = the same through the public API with host buffers, ``roofline`` of
 the sweep, ``cpu_baseline`` (CPU oracle on this host, bounded sample), ``clocks``.
-``--impl reference`` times the reference algorithm's CPU restatement (the oracle) on
-all host cores on a bounded sample of the same workload.
+``--impl reference`` times the reference's own PyTorch CPU path (the unmodified
+``ptychoX`` package installed in ``baseline/_ref`` by ``baseline/install_reference.sh``:
+the operator with ``use_cuda_kernels=False`` in complex64, ``F.mse_loss`` and
+``.backward()``) on all host cores, one whole sweep per step; without that install it
+falls back to the oracle's numpy restatement (``kind: "port"``).
 
 With N > 1 (torchrun) each rank sweeps its own 900 positions over the shared object
 and the gradients are all-reduced over NCCL (data-parallel sweep, weak scaling).
@@ -590,9 +593,15 @@ def run_ours(args) -> None:
                    "observed amplitudes on the device); timed from the first upload to the last read-back"}
 
     # ---- CPU baseline (rank 0, N = 1) --------------------------------------------------
-    cpu = None
+    cpu = cpu_port = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_sample_rate(wl, host, prob["meas"].cpu().numpy(), prob["scale"], budget_s=args.cpu_budget)
+        meas_host = prob["meas"].cpu().numpy()
+        cpu = cpu_reference_rate(wl, host, meas_host, prob["scale"], budget_s=args.cpu_budget)
+        # the oracle's numpy restatement (secondary figure; the primary one when the reference
+        # install is absent)
+        cpu_port = cpu_sample_rate(wl, host, meas_host, prob["scale"], budget_s=args.cpu_budget / 2)
+        if cpu is None:
+            cpu, cpu_port = cpu_port, None
 
     if rank == 0:
         cfg = wl.config()
@@ -614,6 +623,7 @@ def run_ours(args) -> None:
             "config": cfg,
             "roofline": roofline,
             "cpu_baseline": cpu,
+            "cpu_baseline_port": cpu_port,
             "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clk,
@@ -622,6 +632,133 @@ def run_ours(args) -> None:
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+REF_DIR = ROOT / "baseline" / "_ref"
+
+
+def reference_package():
+    """The reference's own ``ptychoX`` package as installed in ``baseline/_ref`` (None when absent).
+
+    ``baseline/install_reference.sh`` pip-installs the unmodified reference there (its CUDA
+    extension built from source for sm_100a) together with its driver scripts, which hold
+    ``fd_loss`` (``train_coded.py:101-107``)."""
+    if not (REF_DIR / "ptychoX" / "__init__.py").exists():
+        return None
+    if str(REF_DIR) not in sys.path:
+        sys.path.insert(0, str(REF_DIR))
+    import ptychoX
+
+    if Path(ptychoX.__file__).resolve().parent.parent != REF_DIR.resolve():
+        raise RuntimeError(f"ptychoX imported from {ptychoX.__file__}, not from {REF_DIR}")
+    return ptychoX
+
+
+def host_threads() -> int:
+    try:
+        return max(1, len(os.sched_getaffinity(0)))
+    except AttributeError:  # pragma: no cover - non-Linux
+        return max(1, os.cpu_count() or 1)
+
+
+def reference_sweep_fn(wl, ref, h, meas, scale, device="cpu", use_cuda_kernels=False):
+    """One whole sweep through the reference's own PyTorch path, as its training drivers run it
+    (``train_ptychography.py:549-557``, ``train_fpm.py:255-263``, ``train_coded.py:225-237``):
+    the operator on complex64 tensors, ``F.mse_loss`` (or ``fd_loss``) against the observed
+    amplitude ``sqrt(scale * counts)``, ``.backward()``.  Returns a callable giving the loss."""
+    import torch
+    import torch.nn.functional as F
+
+    dev = torch.device(device)
+    obj = torch.from_numpy(h["obj"]).to(dev).requires_grad_(True)
+    aux = torch.from_numpy(h["aux"]).to(dev).requires_grad_(True)
+    observed = torch.sqrt(torch.from_numpy(np.asarray(meas).astype(np.float32)).to(dev) * np.float32(scale))
+    loss_fn = F.mse_loss
+    if isinstance(wl, Coded):
+        n = wl.n_obj
+        t1 = (torch.ones((n, n), dtype=torch.complex64, device=dev) if h["t1"] is None
+              else torch.from_numpy(h["t1"]).to(dev))
+        t2 = torch.from_numpy(h["t2"]).to(dev)
+        shifts = torch.from_numpy(np.asarray(h["pos"], dtype=np.float32)).to(dev)
+        if wl.loss != "mse":
+            from train_coded import fd_loss
+
+            iso = wl.loss == "fd-isotropic"
+            loss_fn = lambda a, b: fd_loss(a, b, isotropic=iso)  # noqa: E731
+
+        def forward():
+            return ref.ptychoX_coded(obj, aux, t1, t2, shifts, wl.ds, use_cuda_kernels=use_cuda_kernels)
+    elif isinstance(wl, Fourier):
+        led = torch.from_numpy(np.asarray(h["pos"], dtype=np.int64)).to(dev)
+
+        def forward():
+            return ref.ptychoX_fourier(obj, aux, led, use_cuda_kernels=use_cuda_kernels)
+    else:
+        pos = torch.from_numpy(np.asarray(h["pos"], dtype=np.int64)).to(dev)
+
+        def forward():
+            return ref.ptychoX_base(obj, aux, pos, use_cuda_kernels=use_cuda_kernels)
+
+    def one():
+        obj.grad = None
+        aux.grad = None
+        loss = loss_fn(forward(), observed)
+        loss.backward()
+        return loss.detach()
+
+    return one
+
+
+def reference_counts(wl, ref, h, seed=7):
+    """uint16 Poisson counts of the truth's forward model computed with the reference's own CPU
+    operator (complex64), drawn by numpy; the workload's photon budget."""
+    import torch
+
+    from ptychox_b200 import synth
+
+    t = torch.from_numpy
+    with torch.no_grad():
+        if isinstance(wl, Coded):
+            n = wl.n_obj
+            t1 = torch.ones((n, n), dtype=torch.complex64) if h["t1"] is None else t(h["t1"])
+            amp = ref.ptychoX_coded(t(h["truth"]), t(h["aux"]), t1, t(h["t2"]),
+                                    t(np.asarray(h["pos"], dtype=np.float32)), wl.ds)
+        elif isinstance(wl, Fourier):
+            amp = ref.ptychoX_fourier(t(h["truth"]), t(h["aux"]), t(np.asarray(h["pos"], dtype=np.int64)))
+        else:
+            amp = ref.ptychoX_base(t(h["truth"]), t(h["aux"]), t(np.asarray(h["pos"], dtype=np.int64)))
+    rng = np.random.default_rng(seed)
+    return synth.poisson_counts(amp.numpy().astype(np.float64) ** 2, wl.photons, rng,
+                                per_pixel=isinstance(wl, (Fourier, Coded)), brightest=isinstance(wl, Fourier))
+
+
+def cpu_reference_rate(wl, host, measured, scale, budget_s: float = 12.0) -> dict | None:
+    """Time the reference's own PyTorch CPU path (whole sweeps, all host threads) for about
+    ``budget_s`` seconds after one warm-up sweep; None without the ``baseline/_ref`` install."""
+    import torch
+
+    ref = reference_package()
+    if ref is None:
+        return None
+    threads = host_threads()
+    prev = torch.get_num_threads()
+    torch.set_num_threads(threads)
+    try:
+        one = reference_sweep_fn(wl, ref, host, measured, scale)
+        t0 = time.perf_counter()
+        one()
+        first = time.perf_counter() - t0
+        reps = int(max(1, min(10, budget_s / max(first, 1e-3))))
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            one()
+        dt = (time.perf_counter() - t0) / reps
+    finally:
+        torch.set_num_threads(prev)
+    return {"value": 1.0 / dt, "unit": "sweeps/s", "cores": threads, "kind": "reference",
+            "sample": f"{reps} whole sweeps ({wl.batch} {wl.units} each) after one warm-up sweep; the reference's "
+                      f"ptychoX (baseline/_ref) with use_cuda_kernels=False in complex64 + F.mse_loss + backward, "
+                      f"torch CPU on {threads} threads ({dt:.2f} s per sweep)"}
 
 
 def cpu_sample_rate(wl, host, measured, scale, budget_s: float = 12.0) -> dict:
@@ -653,52 +790,79 @@ def cpu_sample_rate(wl, host, measured, scale, budget_s: float = 12.0) -> dict:
 
 
 def run_reference(args) -> None:
+    """The reference arm: the reference's own PyTorch CPU path on all host threads.
+
+    Each step is one whole sweep (every position) of the workload through the unmodified
+    ``ptychoX`` package of ``baseline/_ref`` (``use_cuda_kernels=False``, complex64,
+    ``F.mse_loss`` + ``.backward()``), on the same seeded problem as our arm.  Without the
+    install the oracle's numpy restatement runs instead, on a bounded sample of the units,
+    and the line says ``kind: "port"``.  Under torchrun only rank 0 runs."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from oracle import ptycho_oracle as O
+    import torch
 
     wl = WORKLOADS[args.workload]
-    workers = O.default_workers()
     h = wl.host(1000)
     batch = wl.batch
-    # a bounded sample per step: enough units for ~2 s of work; counts from the oracle forward
-    rng = np.random.default_rng(7)
+    ref = reference_package()
+    threads = host_threads()
+    if ref is not None:
+        torch.set_num_threads(threads)
+        meas, scale = reference_counts(wl, ref, h)
+        h = dict(h)
+        one = reference_sweep_fn(wl, ref, h, meas, scale)
+        for _ in range(args.warmup):
+            one()
+        times = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            one()
+            times.append(time.perf_counter() - t0)
+        per_sweep = statistics.mean(times)
+        kind = "reference"
+        sample = (f"whole sweeps ({batch} {wl.units} each): the reference's ptychoX from baseline/_ref, "
+                  f"use_cuda_kernels=False, complex64, F.mse_loss + backward, torch CPU on {threads} threads")
+    else:
+        from oracle import ptycho_oracle as O
 
-    def counts(k):
-        if isinstance(wl, Coded):
-            _, _, _, amp = O.coded_forward(h["truth"], h["aux"], h["t1"], h["t2"], h["pos"][:k], wl.ds, fp64=False,
-                                           workers=workers)
-        elif isinstance(wl, Fourier):
-            amp, _, _ = O.fpm_forward(h["truth"], h["aux"], h["pos"][:k], fp64=False, workers=workers)
-        else:
-            amp, _, _ = O.base_forward(h["truth"], h["aux"], h["pos"][:k], fp64=False, workers=workers)
-        from ptychox_b200 import synth
+        workers = O.default_workers()
+        rng = np.random.default_rng(7)
 
-        return synth.poisson_counts(amp.astype(np.float64) ** 2, wl.photons, rng,
-                                    per_pixel=isinstance(wl, (Fourier, Coded)),
-                                    brightest=isinstance(wl, Fourier))
+        def counts(k):
+            if isinstance(wl, Coded):
+                _, _, _, amp = O.coded_forward(h["truth"], h["aux"], h["t1"], h["t2"], h["pos"][:k], wl.ds,
+                                               fp64=False, workers=workers)
+            elif isinstance(wl, Fourier):
+                amp, _, _ = O.fpm_forward(h["truth"], h["aux"], h["pos"][:k], fp64=False, workers=workers)
+            else:
+                amp, _, _ = O.base_forward(h["truth"], h["aux"], h["pos"][:k], fp64=False, workers=workers)
+            from ptychox_b200 import synth
 
-    k = min(batch, 2)
-    meas, scale = counts(k)
-    wl.cpu_sweep(h, meas, scale, k, workers)
-    t0 = time.perf_counter()
-    wl.cpu_sweep(h, meas, scale, k, workers)
-    per_unit = (time.perf_counter() - t0) / k
-    sample = int(min(batch, max(k, 2.0 / max(per_unit, 1e-6))))
-    meas, scale = counts(sample)
+            return synth.poisson_counts(amp.astype(np.float64) ** 2, wl.photons, rng,
+                                        per_pixel=isinstance(wl, (Fourier, Coded)),
+                                        brightest=isinstance(wl, Fourier))
 
-    def one():
-        wl.cpu_sweep(h, meas, scale, sample, workers)
-
-    for _ in range(args.warmup):
-        one()
-    times = []
-    for _ in range(args.steps):
+        k = min(batch, 2)
+        meas, scale = counts(k)
+        wl.cpu_sweep(h, meas, scale, k, workers)
         t0 = time.perf_counter()
-        one()
-        times.append(time.perf_counter() - t0)
-    per_sweep = statistics.mean(times) * batch / sample
+        wl.cpu_sweep(h, meas, scale, k, workers)
+        per_unit = (time.perf_counter() - t0) / k
+        n_units = int(min(batch, max(k, 2.0 / max(per_unit, 1e-6))))
+        meas, scale = counts(n_units)
+        for _ in range(args.warmup):
+            wl.cpu_sweep(h, meas, scale, n_units, workers)
+        times = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            wl.cpu_sweep(h, meas, scale, n_units, workers)
+            times.append(time.perf_counter() - t0)
+        per_sweep = statistics.mean(times) * batch / n_units
+        kind = "port"
+        threads = workers
+        sample = (f"{n_units} of {batch} {wl.units} per step, scaled to one sweep; the oracle's complex64 "
+                  "numpy/scipy restatement of the reference torch CPU path (baseline/_ref not installed)")
     value = 1.0 / per_sweep
     line = {
         "impl": "reference",
@@ -713,11 +877,9 @@ def run_reference(args) -> None:
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "c64",
-        "data": "synthetic (seeded)",
+        "data": "synthetic (seeded object and scan, Poisson uint16 counts from the forward model)",
         "config": wl.config(),
-        "cpu_baseline": {"value": value, "unit": "sweeps/s", "cores": workers, "kind": "port",
-                         "sample": f"{sample} of {batch} {wl.units} per step, scaled to one sweep; complex64 "
-                                   "numpy/scipy restatement of the reference torch CPU path"},
+        "cpu_baseline": {"value": value, "unit": "sweeps/s", "cores": threads, "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": "sweeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

@@ -149,6 +149,18 @@ int ptx_base_sweep_small(const float* sample, int sample_h, int sample_w,
                          double* loss, float* grad_sample, float* grad_probe,
                          void* workspace, size_t workspace_bytes, void* stream);
 
+/* Status word of the last conventional call (ptx_base_forward / _backward / _sweep /
+ * _sweep_small) that used `workspace`: the kernels check every scan window on the device,
+ * skip a frame whose window leaves the object and set bit 0 of the word (the reference reads
+ * such windows out of bounds, base_kernel.cu:108-125; its torch path raises only for windows
+ * past the far edge).  This call copies the 4-byte word in stream order on `stream` to
+ * `status` (device memory or page-locked host memory: no host synchronisation), so a caller
+ * with device-resident positions learns of a bad window without copying the positions to
+ * the host.  Read it after the stream has reached the copy and map it with ptx_status_code. */
+int ptx_workspace_status(const void* workspace, unsigned* status, void* stream);
+/* PTX_ERR_OUT_OF_BOUNDS when bit 0 of a status word is set, else PTX_OK. */
+int ptx_status_code(unsigned status);
+
 /* ---- Fourier ptychography --------------------------------------------------------
  * Operator  A[b] = |ifft2(fftshift(S[window_b] * pupil))|, S = fft2(object), window_b the
  * (lh x lw) block at rows (ly+r+H/2) % H, columns (lx+c+W/2) % W of S.

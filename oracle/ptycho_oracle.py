@@ -51,6 +51,7 @@ __all__ = [
     "base_forward",
     "base_backward",
     "base_sweep",
+    "base_sweep_chunked",
     "fpm_flat_indices",
     "fpm_forward",
     "fpm_backward",
@@ -59,6 +60,7 @@ __all__ = [
     "coded_forward",
     "coded_backward",
     "coded_sweep",
+    "coded_sweep_chunked",
     "nearfield_sweep",
     "default_workers",
     "adam_step",
@@ -214,6 +216,35 @@ def base_sweep(sample, probe, positions_xy, measured_u16, scale, fp64: bool = Tr
     gs, gp = base_backward(g, patches, np.asarray(probe).astype(far.dtype), far, positions_xy,
                            np.asarray(sample).shape, workers)
     return loss, gs, gp
+
+
+def base_sweep_chunked(sample, probe, positions_xy, measured_u16, scale, chunk: int = 64,
+                       workers: int | None = None):
+    """:func:`base_sweep` in FP64, accumulated over chunks of ``chunk`` positions.
+
+    The same sums as the whole-batch sweep (``F.mse_loss`` over all positions, then its
+    backward): the loss sums the squared residuals of every chunk over the total element
+    count, each chunk's adjoint takes ``2 (A - Y) / numel_total`` and the gradients add.
+    Memory stays at one chunk of FP64 far fields (config 1: 900 x 512^2 would need 3.8 GB
+    per whole-batch array).
+    """
+    sample = np.asarray(sample)
+    probe128 = np.asarray(probe).astype(np.complex128)
+    pos = np.asarray(positions_xy, dtype=np.int64).reshape(-1, 2)
+    meas = np.asarray(measured_u16)
+    numel = float(meas.size)
+    total = 0.0
+    gs = np.zeros(sample.shape, np.complex128)
+    gp = np.zeros(probe128.shape, np.complex128)
+    for b0 in range(0, len(pos), chunk):
+        sl = slice(b0, b0 + chunk)
+        amp, far, patches = base_forward(sample, probe, pos[sl], True, workers)
+        diff = amp - measured_amplitude(meas[sl], scale).astype(np.float64)
+        total += float(np.sum(diff * diff))
+        cgs, cgp = base_backward((2.0 / numel) * diff, patches, probe128, far, pos[sl], sample.shape, workers)
+        gs += cgs
+        gp += cgp
+    return total / numel, gs, gp
 
 
 # ----------------------------------------------------------------------------------------
@@ -392,6 +423,36 @@ def coded_sweep(object_field, coded_surface, transfer_1, transfer_2, shifts_xy, 
     out = coded_backward(g, xf, sensor, amp, coded_surface, transfer_1, transfer_2, shifts_xy,
                          downsample, workers, with_shifts=with_shifts)
     return (loss, *out)
+
+
+def coded_sweep_chunked(object_field, coded_surface, transfer_1, transfer_2, shifts_xy, downsample,
+                        measured_u16, scale, chunk: int = 8, fp64: bool = True, workers: int | None = None):
+    """:func:`coded_sweep` (MSE) accumulated over chunks of ``chunk`` shifts.
+
+    Each chunk's adjoint takes ``2 (A - Y) / numel_total``; the object and mask gradients are
+    linear in it, so the chunks' gradients add to the whole-batch result.  ``transfer_1=None``
+    gives the near-field operator.  Memory: one chunk of fields (config 3 holds 64 shifts
+    of 1024^2, 1 GB per whole-batch complex128 array).  ``fp64=False`` runs the complex64
+    formulation (the reference's own FP32 arithmetic) chunk by chunk.
+    """
+    shifts = np.asarray(shifts_xy).reshape(-1, 2)
+    meas = np.asarray(measured_u16)
+    numel = float(meas.size)
+    rd = np.float64 if fp64 else np.float32
+    total = 0.0
+    go = None
+    gm = None
+    for b0 in range(0, len(shifts), chunk):
+        sl = slice(b0, b0 + chunk)
+        _, xf, sensor, amp = coded_forward(object_field, coded_surface, transfer_1, transfer_2, shifts[sl],
+                                           downsample, fp64, workers)
+        diff = amp.astype(rd) - measured_amplitude(meas[sl], scale).astype(rd)
+        total += float(np.sum(diff.astype(np.float64) ** 2))
+        cgo, cgm = coded_backward((rd(2.0 / numel) * diff).astype(rd), xf, sensor, amp, coded_surface, transfer_1,
+                                  transfer_2, shifts[sl], downsample, workers)
+        go = cgo if go is None else go + cgo
+        gm = cgm if gm is None else gm + cgm
+    return total / numel, go, gm
 
 
 def nearfield_sweep(object_field, probe_field, transfer, shifts_xy, downsample, measured_u16, scale,

@@ -5,6 +5,7 @@ operator names, aliases and cache hooks, backed by ``libptychox`` (C ABI in
 ``include/ptychox.h``).  Added: fused forward+loss+adjoint sweeps (``*_loss``).
 """
 
+from ._status import bounds_check_mode, check_errors, set_bounds_check
 from ._utils import matlab_positions_to_torch
 from .base import clear_cuda_plan_cache as clear_base_cuda_plan_cache
 from .base import ptychoX_base, ptychoX_base_loss, ptychography_base
@@ -46,4 +47,7 @@ __all__ = [
     "ptychoX_base_loss",
     "ptychography_base",
     "matlab_positions_to_torch",
+    "set_bounds_check",
+    "bounds_check_mode",
+    "check_errors",
 ]

@@ -68,6 +68,8 @@ SIGNATURES: dict[str, tuple] = {
     "ptx_coded_sweep_ex": (_i, [_p, _p, _p, _p, _i, _p, _i, _i, _p, _f, _i, _p, _p, _p, _p, _p, _sz, _p]),
     "ptx_adam_step": (_i, [_p, _p, _p, _p, _sz, _p, _f, _f, _f, _f, _i, _p]),
     "ptx_base_sweep_noalloc": (_i, [_p, _i, _i, _p, _i, _i, _p, _i, _p, _f, _p, _p, _p, _p]),
+    "ptx_workspace_status": (_i, [_p, _p, _p]),
+    "ptx_status_code": (_i, [C.c_uint]),
     "ptx_reg_workspace_bytes": (_sz, [_i, _i, _i, _i]),
     "ptx_reg_upsampled_peak": (_i, [_p, _i, _i, _i, _i, _p, _p, _p, _p, _p, _sz, _p]),
     "ptx_server_create": (_i, [_i, _sz, _i, _p]),

@@ -60,11 +60,17 @@ def device_positions(
     """int64 contiguous positions on ``device``; windows must lie inside the field.
 
     The reference reads out of bounds for such windows; here they raise ``ValueError``.
+    Host positions are checked on the host before the launch.  Device positions are checked
+    by the kernels themselves and reported through the workspace status word
+    (``_status``: deferred by default, no host synchronisation); only in the ``"host"``
+    bounds-check mode are they copied to the host and checked here.
     """
+    from . import _status
+
     pos = positions_xy.to(dtype=torch.long)
-    if check_bounds and pos.numel():
-        # host positions are checked where they are (no device round trip)
-        host = pos.detach() if pos.device.type == "cpu" else pos.detach().cpu()
+    on_host = pos.device.type == "cpu"
+    if check_bounds and pos.numel() and (on_host or _status.bounds_check_mode() == "host"):
+        host = pos.detach() if on_host else pos.detach().cpu()
         wh, ww = window_hw
         fh, fw = field_hw
         x, y = host[:, 0], host[:, 1]

@@ -14,7 +14,7 @@ from __future__ import annotations
 
 import torch
 
-from . import _abi
+from . import _abi, _status
 from ._utils import (
     as_u16,
     check_complex_scan_inputs,
@@ -60,18 +60,22 @@ def clear_cuda_plan_cache() -> None:
 
 
 def _prepare(sample, probe, positions_xy):
+    """Validated inputs and whether the window check falls to the device (positions that
+    arrive on the device, outside the ``"host"`` bounds-check mode)."""
     check_complex_scan_inputs(sample, probe, positions_xy)
     require_cuda_complex64(("sample", sample), ("probe", probe))
     sample = sample.contiguous()
     probe = probe.contiguous()
+    _status.before_call(sample.device)
     pos = device_positions(positions_xy, sample.device, tuple(probe.shape), tuple(sample.shape))
-    return sample, probe, pos
+    track = positions_xy.device.type != "cpu" and _status.bounds_check_mode() != "host"
+    return sample, probe, pos, track
 
 
 class PtychoXBaseFunction(torch.autograd.Function):
     @staticmethod
     def forward(ctx, sample, probe, positions_xy, use_cuda_kernels=False):  # type: ignore[override]
-        sample, probe, pos = _prepare(sample, probe, positions_xy)
+        sample, probe, pos, track = _prepare(sample, probe, positions_xy)
         dev = sample.device
         batch = pos.shape[0]
         ph, pw = probe.shape
@@ -82,6 +86,8 @@ class PtychoXBaseFunction(torch.autograd.Function):
         with torch.cuda.device(dev):
             _abi.call("ptx_base_forward", ptr(sample), sample.shape[0], sample.shape[1], ptr(probe), ph, pw,
                       ptr(pos), batch, ptr(far), ptr(amp), ptr(ws), ws_bytes, stream_handle(dev))
+            if track and batch:
+                _status.after_call(ws, dev, "ptychoX_base")
         ctx.save_for_backward(sample, probe, far, pos)
         return amp
 
@@ -132,11 +138,16 @@ def base_sweep(sample, probe, positions, measured, scale, ws=None):
 class PtychoXBaseLossFunction(torch.autograd.Function):
     @staticmethod
     def forward(ctx, sample, probe, positions_xy, measured, scale):  # type: ignore[override]
-        sample, probe, pos = _prepare(sample, probe, positions_xy)
+        sample, probe, pos, track = _prepare(sample, probe, positions_xy)
         meas = as_u16(measured, sample.device)
         if tuple(meas.shape) != (pos.shape[0], probe.shape[0], probe.shape[1]):
             raise ValueError("measured must have shape [batch, probe_h, probe_w].")
-        loss, gs, gp = base_sweep(sample, probe, pos, meas, scale)
+        dev = sample.device
+        ws = workspace(_abi.query("ptx_base_workspace_bytes", probe.shape[0], probe.shape[1], pos.shape[0]), dev)
+        loss, gs, gp = base_sweep(sample, probe, pos, meas, scale, ws=ws)
+        if track and pos.shape[0]:
+            with torch.cuda.device(dev):
+                _status.after_call(ws, dev, "ptychoX_base_loss")
         ctx.save_for_backward(gs, gp)
         return loss
 

@@ -751,6 +751,14 @@ struct RegLaunch {
   static int col_smem() { return ColCfg<N>::kSmemBytes; }
 };
 
+// Flag (bit 0 of *err) a window of `pos` that leaves the H x W object.  Used by the adjoint
+// entry point, whose row passes skip such windows without flagging them.
+static __global__ void window_check_kernel(const int64_t* __restrict__ pos, int n, int ph, int pw, int H, int W,
+                                           unsigned* __restrict__ err) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < n && !window_ok(pos[2 * b], pos[2 * b + 1], ph, pw, H, W)) atomicOr(err, 1u);
+}
+
 struct BaseGeom {
   int H, W, ph, pw, batch;
   LinePlan row, col;
@@ -967,6 +975,13 @@ int ptx_base_backward(const float* grad_output, const float* far_field, const fl
   float2* GP = reinterpret_cast<float2*>(grad_probe);
   cudaMemsetAsync(GS, 0, sizeof(float2) * (size_t)sample_h * sample_w, s);
   cudaMemsetAsync(GP, 0, sizeof(float2) * (size_t)probe_h * probe_w, s);
+  cudaMemsetAsync(g.err, 0, sizeof(unsigned), s);
+  if (batch > 0) {
+    prof_begin(kMiscKernel, s);
+    window_check_kernel<<<(batch + 255) / 256, 256, 0, s>>>(positions_xy, batch, probe_h, probe_w, sample_h, sample_w,
+                                                            g.err);
+    prof_end(kMiscKernel, s);
+  }
   const float2* S = reinterpret_cast<const float2*>(sample);
   const float2* P = reinterpret_cast<const float2*>(probe);
   for (int b0 = 0; b0 < batch; b0 += g.chunk) {
@@ -1014,6 +1029,18 @@ int ptx_base_sweep(const float* sample, int sample_h, int sample_w, const float*
   }
   return cuda_status(cudaGetLastError(), "ptx_base_sweep launch");
 }
+
+int ptx_workspace_status(const void* workspace, unsigned* status, void* stream) {
+  if (!workspace || !status) return set_error(PTX_ERR_INVALID_ARGUMENT, "null pointer argument");
+  if (reinterpret_cast<uintptr_t>(workspace) & 255) {
+    return set_error(PTX_ERR_INVALID_ARGUMENT, "workspace must start on a 256-byte boundary");
+  }
+  return cuda_status(cudaMemcpyAsync(status, workspace, sizeof(unsigned), cudaMemcpyDefault,
+                                     static_cast<cudaStream_t>(stream)),
+                     "ptx_workspace_status copy");
+}
+
+int ptx_status_code(unsigned status) { return (status & 1u) ? PTX_ERR_OUT_OF_BOUNDS : PTX_OK; }
 
 int ptx_base_sweep_small(const float* sample, int sample_h, int sample_w, const float* probe, int probe_h,
                          int probe_w, const int64_t* positions_xy, int batch, const uint16_t* measured, float scale,
