@@ -48,7 +48,8 @@ int ptx_version(void);
 /* Message of the calling thread's last failed call ("" if none). */
 const char* ptx_last_error(void);
 
-/* Drop cached FFT plans (twiddle tables are rebuilt on next use).
+/* Drop cached FFT plans (twiddle tables are rebuilt on next use) and the cached device
+ * address of ptx_base_sweep_noalloc's scratch array (looked up again by its next call).
  * Replaces `_C.clear_plan_cache` (base_extension.cpp:65, fpm_extension.cpp:65,
  * coded_extension.cpp:93) and ptychoX.clear_cuda_plan_cache (ptychoX/__init__.py:10-13). */
 int ptx_clear_cache(void);
@@ -64,6 +65,15 @@ long long ptx_launch_count(void);
  * launches made (or captured into CUDA graphs) after the call.  No reference counterpart:
  * the reference's kernels are one-shot grids. */
 int ptx_set_units_per_cta(int units);
+
+/* The same bound for launches made (or captured) by the calling host thread only, overriding
+ * the process-wide value for that thread; units < 0 drops the override.  A server thread that
+ * captures bounded sweeps uses it so that neither the host program's own sweeps nor another
+ * server's captures see its bound.  No reference counterpart. */
+int ptx_set_thread_units_per_cta(int units);
+
+/* The bound in force for the calling thread's launches (its own, else the process-wide one). */
+int ptx_get_units_per_cta(void);
 
 /* Copy `bytes` from host memory `src` (pageable or page-locked) to device memory `dst`
  * (current device) in stream order on `stream`.  Up to 256 KiB the bytes are copied at the
@@ -319,10 +329,9 @@ int ptx_base_sweep_noalloc(const float* sample, int sample_h, int sample_w,
  * stream-ordered allocation), captures one iteration (fused sweep + one Adam step of each
  * parameter) as a CUDA graph with the persistent passes bounded to 8 units per CTA, and
  * replays the iterations of all active reconstructions concurrently on per-reconstruction
- * streams (older ones at higher priority).  While the scheduler captures a reconstruction
- * the process-wide ptx_set_units_per_cta bound is 8 (restored after the capture), so sweeps
- * that other host threads launch at that moment also take bounded units.  Python:
- * ptychox_b200.native_server. */
+ * streams (older ones at higher priority).  The 8-unit bound is the scheduler thread's own
+ * (ptx_set_thread_units_per_cta): the process-wide setting and the sweeps of other host
+ * threads are untouched.  Python: ptychox_b200.native_server. */
 #define PTX_MODALITY_CONVENTIONAL 0
 #define PTX_MODALITY_FOURIER 1
 #define PTX_MODALITY_CODED 2

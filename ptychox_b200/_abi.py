@@ -41,6 +41,8 @@ SIGNATURES: dict[str, tuple] = {
     "ptx_clear_cache": (_i, []),
     "ptx_launch_count": (C.c_longlong, []),
     "ptx_set_units_per_cta": (_i, [_i]),
+    "ptx_set_thread_units_per_cta": (_i, [_i]),
+    "ptx_get_units_per_cta": (_i, []),
     "ptx_stage_host_bytes": (_i, [_p, _p, _sz, _p]),
     "ptx_profile_enable": (_i, [_i]),
     "ptx_profile_reset": (_i, []),

@@ -15,7 +15,10 @@
 //     returns PTX_ERR_WORKSPACE;
 //   - in host code the array's name is not a device address, so the first call on each
 //     device looks the address up with cudaGetSymbolAddress (with that device current)
-//     and caches it; make that first call before any CUDA graph capture;
+//     and caches it; ptx_clear_cache drops the cached addresses (a device reset or a new
+//     primary context gives the array a new address), so the next call looks them up
+//     again; make that first call (and the first after a ptx_clear_cache) before any CUDA
+//     graph capture;
 //   - all calls share the one array: the error word at its start is cleared by each
 //     call and every frame is rewritten before it is read, but calls that overlap on the
 //     GPU (different streams, or different host threads on one device) race on it and
@@ -55,6 +58,12 @@ int noalloc_scratch(void** out) {
 }
 
 }  // namespace
+
+void clear_noalloc_cache() {
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  for (void*& p : g_noalloc_ptr) p = nullptr;
+}
+
 }  // namespace ptx
 
 extern "C" int ptx_base_sweep_noalloc(const float* sample, int sample_h, int sample_w, const float* probe,

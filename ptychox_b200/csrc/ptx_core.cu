@@ -260,15 +260,24 @@ int resident_ctas(const void* kernel, int threads, int smem) {
 }
 
 std::atomic<int> g_units_per_cta{0};
+thread_local int t_units_per_cta = -1;  // this thread's bound (-1: the process-wide one)
+
+int units_per_cta() {
+  return t_units_per_cta >= 0 ? t_units_per_cta : g_units_per_cta.load(std::memory_order_relaxed);
+}
+
+int set_thread_units_per_cta(int units) {
+  const int prev = t_units_per_cta;
+  t_units_per_cta = units < 0 ? -1 : units;
+  return prev;
+}
 
 int persistent_grid(const void* kernel, int threads, int smem, long long units) {
   long long grid = std::min<long long>(units, resident_ctas(kernel, threads, smem));
-  const int k = g_units_per_cta.load(std::memory_order_relaxed);
+  const int k = units_per_cta();
   if (k > 0) grid = std::max(grid, (units + k - 1) / k);
   return static_cast<int>(std::max<long long>(1, std::min<long long>(grid, std::max<long long>(units, 1))));
 }
-
-int units_per_cta() { return g_units_per_cta.load(std::memory_order_relaxed); }
 
 // Device copy of page-locked host memory, read over the bus with loads that never hit a
 // stale cached line of system memory (ld.global.cv).  Grid-stride; 8-byte words when both
@@ -405,6 +414,13 @@ int ptx_set_units_per_cta(int units) {
   return PTX_OK;
 }
 
+int ptx_set_thread_units_per_cta(int units) {
+  ptx::set_thread_units_per_cta(units);
+  return PTX_OK;
+}
+
+int ptx_get_units_per_cta(void) { return ptx::units_per_cta(); }
+
 int ptx_version(void) { return 100; }  // 0.1.0
 
 const char* ptx_last_error(void) { return ptx::g_last_error.c_str(); }
@@ -414,6 +430,7 @@ int ptx_clear_cache(void) {
   // Table offsets stay assigned: a table is rebuilt with identical contents at the same
   // place, so kernels still in flight never see another length's table.
   ptx::g_plans.clear();
+  ptx::clear_noalloc_cache();
   return PTX_OK;
 }
 

@@ -45,6 +45,10 @@ ColShape col_shape(const LinePlan& p);
 
 int sm_count();
 
+// Forget the cached device addresses of the allocation-free sweep's scratch array (looked
+// up again by its next call on each device).
+void clear_noalloc_cache();
+
 // CTAs of `kernel` (launched with `threads` threads and `smem` dynamic shared bytes) that
 // the current device holds at once: SMs x resident CTAs per SM, at least 1.  Cached per
 // (device, kernel, threads, smem).
@@ -53,8 +57,13 @@ int resident_ctas(const void* kernel, int threads, int smem);
 // Grid of a persistent pass over `units` work units: one wave of resident CTAs, or, when
 // ptx_set_units_per_cta(k > 0) is in force, enough CTAs that none takes more than k units.
 int persistent_grid(const void* kernel, int threads, int smem, long long units);
-// The bound set by ptx_set_units_per_cta (0: one wave, no bound).
+// The bound in force for launches of the calling thread: its own bound when one is set
+// (set_thread_units_per_cta), else the process-wide one of ptx_set_units_per_cta (0: one
+// wave, no bound).
 int units_per_cta();
+// Set the calling thread's bound (units >= 0) or drop it (units < 0); returns the previous
+// value (-1 when none was set).
+int set_thread_units_per_cta(int units);
 
 // Kernel kinds for the launch counter and the optional per-kernel event profiler.
 enum KernelId {

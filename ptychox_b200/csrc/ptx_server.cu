@@ -216,8 +216,9 @@ int admit(Slot& s, Request* r, int priority, cudaMemPool_t pool) {
   // one sweep outside the capture builds the FFT plans and kernel attributes
   if (int e = run_sweep(s)) return e;
   if (cudaStreamSynchronize(st) != cudaSuccess) return cuda_status(cudaGetLastError(), "server warm-up");
-  const int saved_units = units_per_cta();
-  ptx_set_units_per_cta(kServerUnitsPerCta);
+  // the bound applies to this (scheduler) thread's launches only: another server's
+  // scheduler, or the host program's own sweeps, keep theirs
+  const int saved_units = set_thread_units_per_cta(kServerUnitsPerCta);
   cudaGraph_t graph = nullptr;
   int status = cuda_status(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "server capture");
   if (!status) {
@@ -225,7 +226,7 @@ int admit(Slot& s, Request* r, int priority, cudaMemPool_t pool) {
     const cudaError_t end = cudaStreamEndCapture(st, &graph);
     if (!status && end != cudaSuccess) status = cuda_status(end, "server capture end");
   }
-  ptx_set_units_per_cta(saved_units);
+  set_thread_units_per_cta(saved_units);
   if (!status && cudaGraphInstantiate(&s.exec, graph, 0) != cudaSuccess) {
     status = cuda_status(cudaGetLastError(), "server graph instantiate");
   }

@@ -222,11 +222,12 @@ class ReconstructionServer:
     def run(self, requests: list[ReconRequest], realtime: bool = True) -> list[ReconResult]:
         """Serve ``requests`` (arrival times in seconds from the start); returns results in rid order."""
         _abi.load()
-        _abi.query("ptx_set_units_per_cta", self.units_per_cta)
+        # the bound covers this thread's launches and captures only (process-wide setting kept)
+        _abi.query("ptx_set_thread_units_per_cta", self.units_per_cta)
         try:
             return self._run(requests, realtime)
         finally:
-            _abi.query("ptx_set_units_per_cta", 0)
+            _abi.query("ptx_set_thread_units_per_cta", -1)
 
     def _run(self, requests: list[ReconRequest], realtime: bool) -> list[ReconResult]:
         pending = sorted(requests, key=lambda r: (r.arrival, r.rid))

@@ -58,6 +58,37 @@ def test_pure_host_entry_points(lib):
     assert lib.ptx_set_units_per_cta(0) == 0
 
 
+def test_thread_units_bound_stays_in_its_thread(lib):
+    """A server thread's capture-time bound (ptx_set_thread_units_per_cta) never leaks into
+    other threads or the process-wide setting, however the threads interleave."""
+    import threading
+
+    barrier = threading.Barrier(2)
+    seen = {}
+
+    def server(name, k):
+        lib.ptx_set_thread_units_per_cta(k)
+        barrier.wait()
+        seen[name] = lib.ptx_get_units_per_cta()
+        barrier.wait()
+        lib.ptx_set_thread_units_per_cta(-1)
+        seen[name + "_after"] = lib.ptx_get_units_per_cta()
+
+    threads = [threading.Thread(target=server, args=(n, k)) for n, k in (("a", 8), ("b", 3))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert seen == {"a": 8, "b": 3, "a_after": 0, "b_after": 0}
+    assert lib.ptx_get_units_per_cta() == 0
+    assert lib.ptx_set_units_per_cta(5) == 0
+    lib.ptx_set_thread_units_per_cta(2)
+    assert lib.ptx_get_units_per_cta() == 2
+    lib.ptx_set_thread_units_per_cta(-1)
+    assert lib.ptx_get_units_per_cta() == 5
+    assert lib.ptx_set_units_per_cta(0) == 0
+
+
 def test_new_entry_points_refuse_bad_arguments_on_the_host(lib):
     """Checks that run before any CUDA call: the small-frame sweep's size rule, the server's
     device and argument checks, the registration workspace query."""

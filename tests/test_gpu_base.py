@@ -295,3 +295,48 @@ def test_config1_finite_differences():
     g_p = np.array([[gp[a, b].real, gp[a, b].imag] for a, b in ppix])
     assert rel_l2(g_o, fd_o) < TOL
     assert rel_l2(g_p, fd_p) < TOL
+
+
+def test_device_window_check_without_host_copy():
+    """Device-resident positions are checked by the kernels: the out-of-object window is
+    reported through the workspace status word (ptx_workspace_status), deferred to the next
+    call or check_errors() by default, at the call itself in "sync" mode."""
+    import ptychox_b200
+    from ptychox_b200 import _abi, ptychoX_base, ptychoX_base_loss
+
+    s = torch.ones(64, 64, dtype=torch.complex64, device="cuda")
+    p = torch.ones(16, 16, dtype=torch.complex64, device="cuda")
+    bad = torch.tensor([[0, 0], [60, 3]], device="cuda")
+    good = torch.tensor([[0, 0], [40, 3]], device="cuda")
+    assert ptychox_b200.bounds_check_mode() == "deferred"
+    out = ptychoX_base(s, p, bad)  # no exception at the call: no host copy, no sync
+    assert out.shape == (2, 16, 16)
+    with pytest.raises(ValueError, match="window leaves the object"):
+        ptychox_b200.check_errors()
+    ptychox_b200.check_errors()  # reported once
+    ptychoX_base(s, p, good)
+    ptychox_b200.check_errors()
+    try:
+        ptychox_b200.set_bounds_check("sync")
+        with pytest.raises(ValueError, match="window leaves the object"):
+            ptychoX_base_loss(s, p, bad, torch.zeros(2, 16, 16, dtype=torch.uint16, device="cuda"), 1.0)
+        ptychox_b200.set_bounds_check("host")
+        with pytest.raises(ValueError, match="window leaves"):
+            ptychoX_base(s, p, bad)
+    finally:
+        ptychox_b200.set_bounds_check("deferred")
+    # the C ABI directly: the word after a sweep over the bad scan, and the code it maps to
+    from ptychox_b200._utils import workspace
+
+    ws = workspace(_abi.query("ptx_base_workspace_bytes", 16, 16, 2), torch.device("cuda"))
+    loss = torch.empty((), dtype=torch.float64, device="cuda")
+    gs, gp = torch.empty_like(s), torch.empty_like(p)
+    meas = torch.zeros(2, 16, 16, dtype=torch.uint16, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    word = torch.full((1,), 7, dtype=torch.int32, device="cuda")
+    for scan, expect in ((bad, 1), (good, 0)):
+        _abi.call("ptx_base_sweep", s.data_ptr(), 64, 64, p.data_ptr(), 16, 16, scan.data_ptr(), 2, meas.data_ptr(),
+                  1.0, loss.data_ptr(), gs.data_ptr(), gp.data_ptr(), ws.data_ptr(), ws.numel(), stream)
+        _abi.call("ptx_workspace_status", ws.data_ptr(), word.data_ptr(), stream)
+        assert int(word.item()) == expect
+        assert _abi.query("ptx_status_code", int(word.item())) == (_abi.PTX_ERR_OUT_OF_BOUNDS if expect else 0)
