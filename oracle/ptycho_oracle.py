@@ -16,6 +16,9 @@ It restates, in numpy/scipy, the PyTorch CPU path of PtychoX
   out step by step in the order of ``coded_kernel.cu:347-424``
 * near-field: the coded operator with ``transfer_1 = 1`` (the MATLAB near-field
   sequence ``fwd_adPtychoX_nearf.cu:58-114`` without the first transfer function)
+* conventional at sub-pixel positions (no reference counterpart): the integer crop of
+  ``base/ops.py:61-62`` at the rounded corner, shifted by the fractional part with
+  ``shift_phase_ramp`` (``coded/ops.py:157-171``), then the conventional operator
 
 plus the amplitude-MSE data term of the training drivers
 (``train_ptychography.py:555``, ``train_fpm.py:261``, ``train_coded.py:235``:
@@ -52,6 +55,10 @@ __all__ = [
     "base_backward",
     "base_sweep",
     "base_sweep_chunked",
+    "subpixel_split",
+    "base_subpix_forward",
+    "base_subpix_backward",
+    "base_subpix_sweep",
     "fpm_flat_indices",
     "fpm_forward",
     "fpm_backward",
@@ -244,6 +251,102 @@ def base_sweep_chunked(sample, probe, positions_xy, measured_u16, scale, chunk: 
         cgs, cgp = base_backward((2.0 / numel) * diff, patches, probe128, far, pos[sl], sample.shape, workers)
         gs += cgs
         gp += cgp
+    return total / numel, gs, gp
+
+
+# ----------------------------------------------------------------------------------------
+# Conventional ptychography at sub-pixel scan positions
+# ----------------------------------------------------------------------------------------
+# The reference crops integer windows only (base/ops.py:61-62).  The sub-pixel operator is
+# composed from its own pieces: the window at the rounded corner (the integer crop), shifted
+# by the fractional part with the reference's Fourier phase ramp (shift_phase_ramp,
+# coded/ops.py:157-171, with the shift in units of the patch side: a band-limited circular
+# shift of the patch), then the conventional forward (base/ops.py:59-67).
+
+
+def subpixel_split(positions_xy):
+    """Integer window corners ``floor(p + 1/2)`` and fractional shifts ``p - corner`` (in
+    [-1/2, 1/2)) of float ``(x, y)`` scan positions."""
+    p = np.asarray(positions_xy, dtype=np.float64).reshape(-1, 2)
+    corner = np.floor(p + 0.5)
+    return corner.astype(np.int64), p - corner
+
+
+def _subpix_ramp(ph, pw, frac, rd):
+    """``exp(2 pi i (dx kx / pw + dy ky / ph))`` per position (the reference's shift_phase_ramp
+    with shifts ``(dx / pw, dy / ph)`` in units of the patch side)."""
+    shifts = np.stack([frac[:, 0] / pw, frac[:, 1] / ph], axis=1)
+    return shift_phase_ramp(ph, pw, shifts, rd)
+
+
+def base_subpix_forward(sample, probe, positions_xy, fp64: bool = True, workers: int | None = None):
+    """``abs(fftshift(fft2(shift(crop(sample)) * probe)))`` at float positions.
+
+    ``shift(C) = ifft2(fft2(C) exp(2 pi i (dx kx / pw + dy ky / ph)))`` samples the cropped
+    window at ``r + (dx, dy)``: position ``(x, y)`` covers the object at ``(x + c, y + r)``.
+    Returns ``(amplitude, far_field_shifted, shifted_patches)``.
+    """
+    cd = _cdtype(fp64, sample, probe)
+    rd = _rdtype(cd)
+    sample = np.asarray(sample).astype(cd, copy=False)
+    probe = np.asarray(probe).astype(cd, copy=False)
+    ph, pw = probe.shape
+    corner, frac = subpixel_split(positions_xy)
+    crops = (np.stack([sample[y : y + ph, x : x + pw] for x, y in corner.tolist()], axis=0) if len(corner)
+             else np.zeros((0, ph, pw), cd))
+    shifted = _ifft2(_fft2(crops, workers) * _subpix_ramp(ph, pw, frac, rd), workers).astype(cd, copy=False)
+    far_field = _fftshift2(_fft2(shifted * probe[None], workers))
+    return np.abs(far_field), far_field, shifted
+
+
+def base_subpix_backward(grad_output, shifted, probe, far_field, positions_xy, sample_shape,
+                         workers: int | None = None):
+    """Adjoint of :func:`base_subpix_forward` (PyTorch's complex-gradient convention).
+
+    ``G = ifft2(ifftshift(g F / max(|F|, eps))) ph pw`` as in ``base/ops.py:92-97``;
+    ``grad_probe = sum_b G conj(S_b)``; the shift is unitary up to ``1/n`` scaling, so its
+    adjoint is the opposite shift: ``grad_C = ifft2(fft2(G conj(probe)) conj(ramp))``,
+    added into the window at the corner.
+    """
+    cd = far_field.dtype
+    rd = _rdtype(cd)
+    ph, pw = probe.shape
+    eps = np.finfo(rd).eps
+    phase = far_field / np.maximum(np.abs(far_field), eps)
+    grad_far = np.asarray(grad_output).astype(rd) * phase
+    grad_exit = _ifft2(_ifftshift2(grad_far), workers) * (ph * pw)
+    grad_probe = np.sum(grad_exit * np.conj(shifted), axis=0).astype(cd)
+    corner, frac = subpixel_split(positions_xy)
+    grad_crop = _ifft2(_fft2(grad_exit * np.conj(probe)[None], workers) * np.conj(_subpix_ramp(ph, pw, frac, rd)),
+                       workers)
+    grad_sample = np.zeros(tuple(sample_shape), dtype=cd)
+    for view, (x, y) in enumerate(corner.tolist()):
+        grad_sample[y : y + ph, x : x + pw] += grad_crop[view]
+    return grad_sample, grad_probe
+
+
+def base_subpix_sweep(sample, probe, positions_xy, measured_u16, scale, fp64: bool = True,
+                      workers: int | None = None, chunk: int | None = None):
+    """Forward, amplitude-MSE loss against decoded counts and adjoint at float positions, the
+    training step of ``train_ptychography.py:549-557`` on the sub-pixel operator.  ``chunk``
+    accumulates over chunks of positions (same sums, bounded memory)."""
+    pos = np.asarray(positions_xy, dtype=np.float64).reshape(-1, 2)
+    meas = np.asarray(measured_u16)
+    probe_c = np.asarray(probe)
+    numel = float(meas.size)
+    step = len(pos) if not chunk else chunk
+    total = 0.0
+    gs = gp = None
+    for b0 in range(0, max(len(pos), 1), max(step, 1)):
+        sl = slice(b0, b0 + step)
+        amp, far, shifted = base_subpix_forward(sample, probe, pos[sl], fp64, workers)
+        rd = np.float64 if fp64 else np.float32
+        diff = amp.astype(rd) - measured_amplitude(meas[sl], scale).astype(rd)
+        total += float(np.sum(diff.astype(np.float64) ** 2))
+        cgs, cgp = base_subpix_backward((rd(2.0 / numel) * diff).astype(rd), shifted, probe_c.astype(far.dtype), far,
+                                        pos[sl], np.asarray(sample).shape, workers)
+        gs = cgs if gs is None else gs + cgs
+        gp = cgp if gp is None else gp + cgp
     return total / numel, gs, gp
 
 

@@ -85,6 +85,19 @@ def raster_positions(grid: int, step: int, origin: int, jitter: int,
     return pos
 
 
+def raster_positions_subpixel(grid: int, step: int, origin: int, jitter: float,
+                              rng: np.random.Generator | None = None, grid_x: int | None = None) -> np.ndarray:
+    """float64 ``[grid*grid_x, 2]`` zero-based ``(x, y)`` raster with real ``U[-j, j]`` jitter
+    (sub-pixel scan positions)."""
+    rng = rng or np.random.default_rng(0)
+    gx = grid if grid_x is None else grid_x
+    ys, xs = np.meshgrid(np.arange(grid), np.arange(gx), indexing="ij")
+    pos = np.stack([origin + xs.ravel() * step, origin + ys.ravel() * step], axis=1).astype(np.float64)
+    if jitter:
+        pos = pos + rng.uniform(-jitter, jitter, size=pos.shape)
+    return pos
+
+
 def poisson_counts(model_intensity: np.ndarray, photons: float, rng: np.random.Generator | None = None,
                    per_pixel: bool = False, brightest: bool = False) -> tuple[np.ndarray, float]:
     """Poisson uint16 counts of ``I / scale`` and the ``scale`` that decodes them.

@@ -15,7 +15,13 @@ It imports ``ptychoX`` from that directory and writes ``tests/golden/*.npz``:
   decoded as ``sqrt(float32(I) * float32(scale))``: loss and gradients;
 * ``sweep_coded_fd_{iso,aniso}_fp64.npz`` — the coded problem with the reference's own
   ``fd_loss`` (``train_coded.py:101-107``, imported from the reference's ``train_coded``
-  module) in place of the MSE.
+  module) in place of the MSE;
+* ``sweep_base_subpix_fp64.npz`` — the conventional sweep at sub-pixel (float) positions,
+  composed from the reference's crop, ``shift_phase_ramp`` (``coded/ops.py:157-171``) and
+  ``ptychoX_base`` (the reference has no sub-pixel operator of its own).
+
+``REFERENCE_PYTHON_DIR`` is required; a second argument ``fd``, ``shifts`` or ``subpix``
+regenerates only that family.
 
 The fixtures are small (a few hundred KB in total) and are the parity pin of the
 numpy oracle (``oracle/``) and of the CUDA library.
@@ -111,6 +117,46 @@ def sweep_base(ptychoX, name, n_obj, ph, pw, grid, step, origin, jitter, photons
                                         _observed(counts, scale))
     np.savez(HERE / name, sample=obj, probe=probe, positions=pos, measured=counts, scale=np.float32(scale),
              loss=loss, grad_sample=g_obj, grad_probe=g_probe)
+
+
+def sweep_base_subpix(ptychoX, name, n_obj, ph, pw, grid, step, origin, jitter, photons, seed):
+    """Conventional sweep at sub-pixel positions, composed from the reference's own functions
+    (it has no sub-pixel operator): the crop of base/ops.py:61-62 at the rounded corner
+    floor(p + 1/2), the fractional shift by shift_phase_ramp (coded/ops.py:157-171, shifts in
+    units of the patch side) applied to the patch's spectrum, and ptychoX_base on the shifted
+    patch (its own sample, position (0, 0)); autograd takes the gradients through it all."""
+    from ptychoX.coded.ops import shift_phase_ramp
+
+    rng = np.random.default_rng(seed)
+    obj_true = synth.random_object(n_obj, n_obj, rng)
+    probe_true = synth.gaussian_probe(ph, pw, rng)
+    pos = synth.raster_positions_subpixel(grid, step, origin, jitter, rng)
+    corner = np.floor(pos + 0.5)
+    frac = pos - corner
+    shifts = torch.from_numpy(np.stack([frac[:, 0] / pw, frac[:, 1] / ph], axis=1))
+    zero = torch.zeros(1, 2, dtype=torch.long)
+
+    def forward(o, pr):
+        ramp = shift_phase_ramp(ph, pw, shifts, o.device, torch.float64)
+        outs = []
+        for b, (x, y) in enumerate(corner.astype(np.int64).tolist()):
+            crop = o[y : y + ph, x : x + pw]
+            patch = torch.fft.ifft2(torch.fft.fft2(crop) * ramp[b])
+            outs.append(ptychoX.ptychoX_base(patch, pr, zero))
+        return torch.cat(outs, dim=0)
+
+    with torch.no_grad():
+        amp = forward(torch.from_numpy(obj_true.astype(np.complex128)), torch.from_numpy(probe_true.astype(np.complex128)))
+    counts, scale = synth.poisson_counts(_np(amp) ** 2, photons, rng)
+    obj = (obj_true * (1.0 + 0.15 * rng.standard_normal(obj_true.shape))).astype(np.complex64)
+    probe = (probe_true * np.exp(0.2j * rng.standard_normal(probe_true.shape))).astype(np.complex64)
+    loss, (g_obj, g_probe) = _loss_step(forward, [obj, probe], _observed(counts, scale))
+    np.savez(HERE / name, sample=obj, probe=probe, positions=pos, measured=counts, scale=np.float32(scale),
+             loss=loss, grad_sample=g_obj, grad_probe=g_probe)
+
+
+def subpix_case(ptychoX):
+    sweep_base_subpix(ptychoX, "sweep_base_subpix_fp64.npz", 96, 16, 32, 4, 12, 6, 2.5, 1e4, seed=17)
 
 
 def sweep_fpm(ptychoX, name, n, h, leds_grid, photons, seed):
@@ -215,15 +261,18 @@ def main(ref_python_dir: str) -> None:
     sweep_coded(ptychoX, "sweep_nearfield_fp64.npz", 32, 4, 3, 200.0, seed=15, nearfield=True)
     fd_cases(ptychoX)
     shift_case(ptychoX)
+    subpix_case(ptychoX)
     print("wrote", sorted(p.name for p in HERE.glob("*.npz")))
 
 
 if __name__ == "__main__":
-    if len(sys.argv) > 2 and sys.argv[2] in ("fd", "shifts"):  # only the fd_loss / shift fixtures
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_golden.py REFERENCE_PYTHON_DIR [fd|shifts|subpix]")
+    if len(sys.argv) > 2 and sys.argv[2] in ("fd", "shifts", "subpix"):  # one family of fixtures only
         sys.dont_write_bytecode = True
         sys.path.insert(0, sys.argv[1])
         import ptychoX  # noqa: E402
 
-        fd_cases(ptychoX) if sys.argv[2] == "fd" else shift_case(ptychoX)
+        {"fd": fd_cases, "shifts": shift_case, "subpix": subpix_case}[sys.argv[2]](ptychoX)
     else:
-        main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/python")
+        main(sys.argv[1])

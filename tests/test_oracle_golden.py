@@ -106,3 +106,27 @@ def test_coded_shift_gradient():
     assert rel_l2(go, g["grad_object"]) < TOL_F64
     assert rel_l2(gm, g["grad_mask"]) < TOL_F64
     assert rel_l2(gs, g["grad_shifts"]) < TOL_F64
+
+
+def test_sweep_base_subpixel():
+    """Sub-pixel conventional sweep: the oracle against the fixture composed from the reference's
+    own crop, shift_phase_ramp and ptychoX_base (rectangular 16 x 32 probe, real jitter)."""
+    g = load_golden("sweep_base_subpix_fp64.npz")
+    assert np.any(np.abs(g["positions"] - np.round(g["positions"])) > 0.1)
+    loss, gs, gp = O.base_subpix_sweep(g["sample"], g["probe"], g["positions"], g["measured"], float(g["scale"]))
+    assert abs(loss - float(g["loss"])) <= TOL_F64 * abs(float(g["loss"]))
+    assert rel_l2(gs, g["grad_sample"]) < TOL_F64
+    assert rel_l2(gp, g["grad_probe"]) < TOL_F64
+    chunked = O.base_subpix_sweep(g["sample"], g["probe"], g["positions"], g["measured"], float(g["scale"]), chunk=5)
+    assert abs(chunked[0] - loss) <= 1e-12 * abs(loss)
+    assert rel_l2(chunked[1], gs) < 1e-12 and rel_l2(chunked[2], gp) < 1e-12
+
+
+def test_subpixel_integer_positions_equal_base():
+    """At integer positions the sub-pixel operator is the conventional one."""
+    g = load_golden("sweep_base_fp64.npz")
+    pos = g["positions"].astype(np.float64)
+    a = O.base_sweep(g["sample"], g["probe"], g["positions"], g["measured"], float(g["scale"]))
+    b = O.base_subpix_sweep(g["sample"], g["probe"], pos, g["measured"], float(g["scale"]))
+    assert abs(a[0] - b[0]) <= 1e-12 * abs(a[0])
+    assert rel_l2(b[1], a[1]) < 1e-12 and rel_l2(b[2], a[2]) < 1e-12
