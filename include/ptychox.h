@@ -171,6 +171,49 @@ int ptx_workspace_status(const void* workspace, unsigned* status, void* stream);
 /* PTX_ERR_OUT_OF_BOUNDS when bit 0 of a status word is set, else PTX_OK. */
 int ptx_status_code(unsigned status);
 
+/* ---- conventional ptychography at sub-pixel scan positions -------------------------
+ * No reference counterpart: the reference crops integer windows only
+ * (python/ptychoX/base/ops.py:61-62, base_extension.cpp:30 demands int64).  positions_xy
+ * holds float64 (x, y) pairs; each frame takes the window at the rounded corner
+ * (x0, y0) = floor(p + 1/2) and shifts it by the fraction (dx, dy) = p - (x0, y0) in
+ * [-1/2, 1/2) with the Fourier phase ramp of the reference's shift_phase_ramp
+ * (coded/ops.py:157-171) applied to the patch:
+ *   S = ifft2(fft2(O[y0:y0+ph, x0:x0+pw]) exp(2 pi i (dx kx / pw + dy ky / ph))),
+ *   A = |fftshift(fft2(S * probe))|
+ * (kx, ky the signed integer frequencies).  At integer positions S is the plain window.
+ * Probe sides: powers of two in [16, 1024] (PTX_ERR_UNSUPPORTED_SIZE otherwise).  Windows that
+ * leave the object are skipped and flagged in the status word (ptx_workspace_status).
+ * Workspace: ptx_base_subpix_workspace_bytes (tables of the per-frame ramps, and two scratch
+ * frames per frame processed at once). */
+size_t ptx_base_subpix_workspace_bytes(int probe_h, int probe_w, int batch);
+
+/* Forward: far_field (complex64 [batch, ph, pw], fftshifted, may be NULL) and amplitude. */
+int ptx_base_subpix_forward(const float* sample, int sample_h, int sample_w,
+                            const float* probe, int probe_h, int probe_w,
+                            const double* positions_xy, int batch,
+                            float* far_field, float* amplitude,
+                            void* workspace, size_t workspace_bytes, void* stream);
+
+/* Adjoint for grad_output (float32 [batch, ph, pw]) from the forward's far field;
+ * grad_sample and grad_probe are OVERWRITTEN. */
+int ptx_base_subpix_backward(const float* grad_output, const float* far_field,
+                             const float* sample, int sample_h, int sample_w,
+                             const float* probe, int probe_h, int probe_w,
+                             const double* positions_xy, int batch,
+                             float* grad_sample, float* grad_probe,
+                             void* workspace, size_t workspace_bytes, void* stream);
+
+/* Fused sweep: mean((A - sqrt(scale * I))^2) in FP64 and its gradients (OVERWRITTEN), as
+ * ptx_base_sweep on the sub-pixel operator (five passes: column shift of the gathered
+ * window, row shift x probe x row DFT, the column loss pass, the row adjoint with the probe
+ * gradient, the column adjoint with the object scatter). */
+int ptx_base_subpix_sweep(const float* sample, int sample_h, int sample_w,
+                          const float* probe, int probe_h, int probe_w,
+                          const double* positions_xy, int batch,
+                          const uint16_t* measured, float scale,
+                          double* loss, float* grad_sample, float* grad_probe,
+                          void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---- Fourier ptychography --------------------------------------------------------
  * Operator  A[b] = |ifft2(fftshift(S[window_b] * pupil))|, S = fft2(object), window_b the
  * (lh x lw) block at rows (ly+r+H/2) % H, columns (lx+c+W/2) % W of S.

@@ -8,7 +8,13 @@ operator names, aliases and cache hooks, backed by ``libptychox`` (C ABI in
 from ._status import bounds_check_mode, check_errors, set_bounds_check
 from ._utils import matlab_positions_to_torch
 from .base import clear_cuda_plan_cache as clear_base_cuda_plan_cache
-from .base import ptychoX_base, ptychoX_base_loss, ptychography_base
+from .base import (
+    ptychoX_base,
+    ptychoX_base_loss,
+    ptychoX_base_subpixel,
+    ptychoX_base_subpixel_loss,
+    ptychography_base,
+)
 from .coded import clear_cuda_plan_cache as clear_coded_cuda_plan_cache
 from .coded import (
     coded_ptychography,
@@ -45,6 +51,8 @@ __all__ = [
     "fourier_ptychography",
     "ptychoX_base",
     "ptychoX_base_loss",
+    "ptychoX_base_subpixel",
+    "ptychoX_base_subpixel_loss",
     "ptychography_base",
     "matlab_positions_to_torch",
     "set_bounds_check",

@@ -56,6 +56,10 @@ SIGNATURES: dict[str, tuple] = {
     "ptx_base_backward": (_i, [_p, _p, _p, _i, _i, _p, _i, _i, _p, _i, _p, _p, _p, _sz, _p]),
     "ptx_base_sweep": (_i, [_p, _i, _i, _p, _i, _i, _p, _i, _p, _f, _p, _p, _p, _p, _sz, _p]),
     "ptx_base_sweep_small": (_i, [_p, _i, _i, _p, _i, _i, _p, _i, _p, _f, _p, _p, _p, _p, _sz, _p]),
+    "ptx_base_subpix_workspace_bytes": (_sz, [_i, _i, _i]),
+    "ptx_base_subpix_forward": (_i, [_p, _i, _i, _p, _i, _i, _p, _i, _p, _p, _p, _sz, _p]),
+    "ptx_base_subpix_backward": (_i, [_p, _p, _p, _i, _i, _p, _i, _i, _p, _i, _p, _p, _p, _sz, _p]),
+    "ptx_base_subpix_sweep": (_i, [_p, _i, _i, _p, _i, _i, _p, _i, _p, _f, _p, _p, _p, _p, _sz, _p]),
     "ptx_fpm_workspace_bytes": (_sz, [_i, _i, _i, _i, _i]),
     "ptx_fpm_forward": (_i, [_p, _i, _i, _p, _i, _i, _p, _i, _p, _p, _p, _p, _sz, _p]),
     "ptx_fpm_backward": (_i, [_p, _p, _p, _i, _i, _p, _i, _i, _p, _i, _p, _p, _p, _sz, _p]),

@@ -79,6 +79,33 @@ def device_positions(
     return upload_small(pos, device, torch.long)
 
 
+def device_positions_subpixel(
+    positions_xy: torch.Tensor,
+    device: torch.device,
+    window_hw: tuple[int, int],
+    field_hw: tuple[int, int],
+    name: str = "positions_xy",
+) -> torch.Tensor:
+    """float64 contiguous sub-pixel positions on ``device``.  Each window starts at the rounded
+    corner ``floor(p + 1/2)``; host positions are checked here as in :func:`device_positions`,
+    device positions by the kernels (the workspace status word)."""
+    from . import _status
+
+    pos = positions_xy.to(dtype=torch.float64)
+    on_host = pos.device.type == "cpu"
+    if pos.numel() and (on_host or _status.bounds_check_mode() == "host"):
+        host = pos.detach() if on_host else pos.detach().cpu()
+        if not bool(torch.isfinite(host).all()):
+            raise ValueError(f"{name} must be finite.")
+        corner = torch.floor(host + 0.5)
+        wh, ww = window_hw
+        fh, fw = field_hw
+        x, y = corner[:, 0], corner[:, 1]
+        if bool((x < 0).any() or (y < 0).any() or (x + ww > fw).any() or (y + wh > fh).any()):
+            raise ValueError(f"{name}: a {wh}x{ww} window leaves the {fh}x{fw} field.")
+    return upload_small(pos, device, torch.float64)
+
+
 def upload_small(t: torch.Tensor, device: torch.device, dtype: torch.dtype) -> torch.Tensor:
     """``t`` as a contiguous ``dtype`` tensor on ``device``, in order on the current stream.
 

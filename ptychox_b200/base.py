@@ -19,6 +19,7 @@ from ._utils import (
     as_u16,
     check_complex_scan_inputs,
     device_positions,
+    device_positions_subpixel,
     ptr,
     require_cuda_complex64,
     stream_handle,
@@ -29,6 +30,8 @@ __all__ = [
     "ptychoX_base",
     "ptychography_base",
     "ptychoX_base_loss",
+    "ptychoX_base_subpixel",
+    "ptychoX_base_subpixel_loss",
     "clear_cuda_plan_cache",
     "PtychoXBaseFunction",
     "PtychoXBaseLossFunction",
@@ -172,3 +175,128 @@ def ptychoX_base_loss(
     ``sample.grad`` / ``probe.grad`` exactly as the unfused composition does.
     """
     return PtychoXBaseLossFunction.apply(sample, probe, positions_xy, measured, scale)
+
+
+# ---------------------------------------------------------------------------------------
+# Sub-pixel scan positions (no reference counterpart: the reference crops integer windows,
+# base/ops.py:61-62).  A float position (x, y) takes the window at floor(p + 1/2) and shifts
+# it by the fraction with the reference's Fourier phase ramp (coded/ops.py:157-171).
+# ---------------------------------------------------------------------------------------
+
+
+def _prepare_subpixel(sample, probe, positions_xy):
+    check_complex_scan_inputs(sample, probe, positions_xy)
+    require_cuda_complex64(("sample", sample), ("probe", probe))
+    sample = sample.contiguous()
+    probe = probe.contiguous()
+    _status.before_call(sample.device)
+    pos = device_positions_subpixel(positions_xy, sample.device, tuple(probe.shape), tuple(sample.shape))
+    track = positions_xy.device.type != "cpu" and _status.bounds_check_mode() != "host"
+    return sample, probe, pos, track
+
+
+def _subpixel_ws_bytes(ph, pw, batch):
+    n = _abi.query("ptx_base_subpix_workspace_bytes", ph, pw, batch)
+    if n == 0:
+        raise ValueError(f"sub-pixel scans take probe sides that are powers of two in [16, 1024] (got {ph}x{pw}).")
+    return n
+
+
+def base_subpixel_sweep(sample, probe, positions, measured, scale, ws=None):
+    """One fused sub-pixel sweep on validated device tensors (``positions`` float64 on the
+    device); returns ``(loss, grad_sample, grad_probe)``."""
+    dev = sample.device
+    batch = positions.shape[0]
+    ph, pw = probe.shape
+    loss = torch.empty((), dtype=torch.float64, device=dev)
+    gs = torch.empty_like(sample)
+    gp = torch.empty_like(probe)
+    if ws is None:
+        ws = workspace(_subpixel_ws_bytes(ph, pw, batch), dev)
+    with torch.cuda.device(dev):
+        _abi.call("ptx_base_subpix_sweep", ptr(sample), sample.shape[0], sample.shape[1], ptr(probe), ph, pw,
+                  ptr(positions), batch, ptr(measured), float(scale), ptr(loss), ptr(gs), ptr(gp), ptr(ws), ws.numel(),
+                  stream_handle(dev))
+    return loss, gs, gp
+
+
+class PtychoXBaseSubpixelFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, sample, probe, positions_xy):  # type: ignore[override]
+        sample, probe, pos, track = _prepare_subpixel(sample, probe, positions_xy)
+        dev = sample.device
+        batch = pos.shape[0]
+        ph, pw = probe.shape
+        far = torch.empty((batch, ph, pw), dtype=torch.complex64, device=dev)
+        amp = torch.empty((batch, ph, pw), dtype=torch.float32, device=dev)
+        ws_bytes = _subpixel_ws_bytes(ph, pw, batch)
+        ws = workspace(ws_bytes, dev)
+        with torch.cuda.device(dev):
+            _abi.call("ptx_base_subpix_forward", ptr(sample), sample.shape[0], sample.shape[1], ptr(probe), ph, pw,
+                      ptr(pos), batch, ptr(far), ptr(amp), ptr(ws), ws_bytes, stream_handle(dev))
+            if track and batch:
+                _status.after_call(ws, dev, "ptychoX_base_subpixel")
+        ctx.save_for_backward(sample, probe, far, pos)
+        return amp
+
+    @staticmethod
+    def backward(ctx, grad_output):  # type: ignore[override]
+        sample, probe, far, pos = ctx.saved_tensors
+        dev = sample.device
+        batch = pos.shape[0]
+        ph, pw = probe.shape
+        grad_output = grad_output.to(dtype=torch.float32).contiguous()
+        grad_sample = torch.empty_like(sample)
+        grad_probe = torch.empty_like(probe)
+        ws_bytes = _subpixel_ws_bytes(ph, pw, batch)
+        ws = workspace(ws_bytes, dev)
+        with torch.cuda.device(dev):
+            _abi.call("ptx_base_subpix_backward", ptr(grad_output), ptr(far), ptr(sample), sample.shape[0],
+                      sample.shape[1], ptr(probe), ph, pw, ptr(pos), batch, ptr(grad_sample), ptr(grad_probe),
+                      ptr(ws), ws_bytes, stream_handle(dev))
+        return grad_sample, grad_probe, None
+
+
+class PtychoXBaseSubpixelLossFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, sample, probe, positions_xy, measured, scale):  # type: ignore[override]
+        sample, probe, pos, track = _prepare_subpixel(sample, probe, positions_xy)
+        meas = as_u16(measured, sample.device)
+        ph, pw = probe.shape
+        if tuple(meas.shape) != (pos.shape[0], ph, pw):
+            raise ValueError("measured must have shape [batch, probe_h, probe_w].")
+        dev = sample.device
+        ws = workspace(_subpixel_ws_bytes(ph, pw, pos.shape[0]), dev)
+        loss, gs, gp = base_subpixel_sweep(sample, probe, pos, meas, scale, ws=ws)
+        if track and pos.shape[0]:
+            with torch.cuda.device(dev):
+                _status.after_call(ws, dev, "ptychoX_base_subpixel_loss")
+        ctx.save_for_backward(gs, gp)
+        return loss
+
+    @staticmethod
+    def backward(ctx, grad_loss):  # type: ignore[override]
+        gs, gp = ctx.saved_tensors
+        g = grad_loss.to(torch.float32)
+        return gs * g, gp * g, None, None, None
+
+
+def ptychoX_base_subpixel(sample: torch.Tensor, probe: torch.Tensor, positions_xy: torch.Tensor) -> torch.Tensor:
+    """``abs(fftshift(fft2(shift(crop(sample)) * probe)))`` at float scan positions.
+
+    ``positions_xy``: ``[batch, 2]`` zero-based ``(x, y)``, any real dtype (kept in float64).
+    Each frame crops the window at ``floor(p + 1/2)`` and shifts it by the fractional part
+    with a Fourier phase ramp (the reference's ``shift_phase_ramp``, ``coded/ops.py:157-171``,
+    applied to the patch), so ``(x, y)`` samples the object at ``(x + c, y + r)``.  At
+    integer positions this is :func:`ptychoX_base`.  Probe sides: powers of two in [16, 1024].
+    Differentiable in ``sample`` and ``probe``.
+    """
+    return PtychoXBaseSubpixelFunction.apply(sample, probe, positions_xy)
+
+
+def ptychoX_base_subpixel_loss(sample: torch.Tensor, probe: torch.Tensor, positions_xy: torch.Tensor,
+                               measured: torch.Tensor, scale: float) -> torch.Tensor:
+    """Fused ``F.mse_loss(ptychoX_base_subpixel(sample, probe, positions), sqrt(scale * measured))``:
+    one five-pass sweep, an FP64 scalar whose ``.backward()`` fills ``sample.grad`` and
+    ``probe.grad``."""
+    return PtychoXBaseSubpixelLossFunction.apply(sample, probe, positions_xy, measured, scale)

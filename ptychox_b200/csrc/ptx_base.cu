@@ -922,6 +922,36 @@ void launch_cols(const BaseGeom& g, int frame0, int nframes, const uint16_t* mea
 }
 
 }  // namespace
+
+int base_cols_pass(bool forward, float2* scratch, int ph, int pw, int frame0, int nframes, float2* far_field,
+                   float* amplitude, const float* grad_output, cudaStream_t s) {
+  BaseGeom g{};
+  g.ph = ph;
+  g.pw = pw;
+  g.scratch = scratch;
+  if (int st = get_line_plan(ph, &g.col)) return st;
+  g.cs = col_shape(g.col);
+  int st = PTX_OK;
+  dispatch_len(ph, [&](auto NT) {
+    constexpr int N = decltype(NT)::value;
+    if constexpr (N > 0) {
+      const int sm = RegLaunch<N>::col_smem();
+      st = ensure_smem(forward ? (const void*)base_cols_reg<kColForward, N> : (const void*)base_cols_reg<kColBackward, N>,
+                       sm);
+    } else {
+      st = ensure_smem(forward ? (const void*)base_cols_rt<kColForward, 0> : (const void*)base_cols_rt<kColBackward, 0>,
+                       g.cs.smem);
+    }
+  });
+  if (st) return st;
+  if (forward) {
+    launch_cols<kColForward>(g, frame0, nframes, nullptr, 0.f, 0.f, 0.0, nullptr, far_field, amplitude, nullptr, s);
+  } else {
+    launch_cols<kColBackward>(g, frame0, nframes, nullptr, 0.f, 0.f, 0.0, nullptr, far_field, nullptr, grad_output, s);
+  }
+  return PTX_OK;
+}
+
 }  // namespace ptx
 
 using namespace ptx;

@@ -175,7 +175,8 @@ ColShape col_shape(const LinePlan& p) {
 namespace {
 const char* const kKernelNames[kNumKernelIds] = {
     "base_rows_forward", "base_cols", "base_rows_adjoint", "fpm_rows_forward", "fpm_cols",
-    "fpm_rows_adjoint", "fft2_rows", "fft2_cols", "coded_rows", "coded_cols", "misc"};
+    "fpm_rows_adjoint", "fft2_rows", "fft2_cols", "coded_rows", "coded_cols", "misc",
+    "subpix_cols",      "subpix_rows"};
 
 struct Profiler {
   std::mutex mu;
@@ -421,7 +422,7 @@ int ptx_set_thread_units_per_cta(int units) {
 
 int ptx_get_units_per_cta(void) { return ptx::units_per_cta(); }
 
-int ptx_version(void) { return 100; }  // 0.1.0
+int ptx_version(void) { return 200; }  // 0.2.0
 
 const char* ptx_last_error(void) { return ptx::g_last_error.c_str(); }
 

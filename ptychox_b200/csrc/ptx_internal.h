@@ -45,6 +45,13 @@ ColShape col_shape(const LinePlan& p);
 
 int sm_count();
 
+// Column pass of the conventional operator over `nframes` tiled scratch frames ([tile][row][16],
+// ph x pw) whose counts / far fields start at frame `frame0`: forward (column DFT; the fftshifted
+// far field, when non-null, and the amplitude) or backward (g F / max(|F|, eps) from the saved
+// far field, inverse column DFT into the frames).
+int base_cols_pass(bool forward, float2* scratch, int ph, int pw, int frame0, int nframes, float2* far_field,
+                   float* amplitude, const float* grad_output, cudaStream_t s);
+
 // Forget the cached device addresses of the allocation-free sweep's scratch array (looked
 // up again by its next call on each device).
 void clear_noalloc_cache();
@@ -78,6 +85,8 @@ enum KernelId {
   kCodedRows,
   kCodedCols,
   kMiscKernel,
+  kSubpixCols,
+  kSubpixRows,
   kNumKernelIds
 };
 // Call around every kernel launch: counts launches and, when profiling is on, records
