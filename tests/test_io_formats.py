@@ -35,3 +35,33 @@ def test_round_trip(tmp_path):
         assert d[k_obj].dtype == torch.complex64 and np.array_equal(d[k_obj].numpy(), obj)
         assert np.array_equal(d[k_aux].numpy(), aux) and np.array_equal(d[k_scan].numpy(), pos)
         assert np.array_equal(d["observed_amplitude"].numpy(), amp) and d["args"] == {"lr": 0.1}
+
+
+def test_matlab_dataset_round_trip(tmp_path):
+    """imgRawData.mat as gen_img.m:59 writes it: imRaw [h, w, n] (MATLAB order), ScanPos [n, 2],
+    pattern, env struct; read back into [n, h, w] and the near-field arguments."""
+    from scipy.io import loadmat
+
+    from ptychox_b200 import io
+
+    rng = np.random.default_rng(0)
+    n, pix, mag = 3, 8, 4
+    raw = rng.random((n, pix, pix)) * 5 + 1
+    pos = rng.uniform(-17, 17, size=(n, 2))
+    pattern = (rng.standard_normal((pix * mag, pix * mag)) + 1j * rng.standard_normal((pix * mag, pix * mag)))
+    env = {"Fx": rng.random((pix * mag, pix * mag)), "pixSz": 5.86 / mag, "size": np.array([pix * mag, pix * mag])}
+    path = io.save_matlab_dataset(tmp_path / "imgRawData.mat", raw, pos, pattern, env)
+    m = loadmat(str(path))
+    assert m["imRaw"].shape == (pix, pix, n)
+    assert np.allclose(m["imRaw"][:, :, 1], raw[1])
+    assert m["ScanPos"].shape == (n, 2)
+    d = io.load_matlab_dataset(path)
+    assert np.allclose(d["im_raw"], raw) and np.allclose(d["scan_pos"], pos)
+    assert np.allclose(d["pattern"], pattern.astype(np.complex64))
+    assert np.isclose(float(d["env"]["pixSz"]), 5.86 / mag) and np.allclose(d["env"]["Fx"], env["Fx"])
+    args = io.nearfield_inputs(d)
+    assert args["downsample"] == mag
+    assert args["measured"].dtype == np.uint16 and args["measured"].max() == 65535
+    assert np.allclose(args["shifts_xy"], pos / pix, atol=1e-6)
+    norm = (raw - raw.min()) / (raw - raw.min()).max()
+    assert np.max(np.abs(args["measured"] * args["scale"] - norm)) <= 0.5 * args["scale"] + 1e-7
