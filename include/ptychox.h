@@ -372,9 +372,15 @@ int ptx_base_sweep_noalloc(const float* sample, int sample_h, int sample_w,
  * stream-ordered allocation), captures one iteration (fused sweep + one Adam step of each
  * parameter) as a CUDA graph with the persistent passes bounded to 8 units per CTA, and
  * replays the iterations of all active reconstructions concurrently on per-reconstruction
- * streams (older ones at higher priority).  The 8-unit bound is the scheduler thread's own
- * (ptx_set_thread_units_per_cta): the process-wide setting and the sweeps of other host
- * threads are untouched.  Python: ptychox_b200.native_server. */
+ * streams (older ones at higher priority).  Two threads: the scheduler thread only queues
+ * graph replays and polls events (it never waits on the device); an admission thread does
+ * the blocking work -- allocation, upload, the warm-up sweep, capture, and the read-back of
+ * finished reconstructions -- off the scheduler's path.  The 8-unit bound is the capturing
+ * thread's own (ptx_set_thread_units_per_cta): the process-wide setting and the sweeps of
+ * other host threads are untouched.  A request with target_ratio > 0 stops at a fixed error:
+ * once a completed iteration's loss is at most target_ratio times the initial loss (the
+ * sweep at obj0 / aux0), no further iteration is queued.  Python:
+ * ptychox_b200.native_server. */
 #define PTX_MODALITY_CONVENTIONAL 0
 #define PTX_MODALITY_FOURIER 1
 #define PTX_MODALITY_CODED 2
@@ -396,6 +402,7 @@ typedef struct ptx_recon_request {
   const uint16_t* measured;  /* host counts [batch][aux_h][aux_w], coded [batch][n/ds][n/ds] */
   const float* transfer_1; /* host complex64 [n][n] (coded; NULL otherwise) */
   const float* transfer_2; /* host complex64 [n][n] (coded and near-field) */
+  float target_ratio;      /* > 0: stop once loss <= target_ratio * initial loss; 0: run all iters */
 } ptx_recon_request;
 
 /* Start a server on `device`; hbm_budget 0 = 70% of the free device memory. */
@@ -410,6 +417,10 @@ int ptx_server_submit(void* server, const ptx_recon_request* request, long long*
  * forgotten.  A failed request returns its error code (and is forgotten). */
 int ptx_server_poll(void* server, long long id, int* done, double* final_loss, double* latency_s,
                     float* object_out, float* aux_out);
+/* ptx_server_poll that also reports the iterations the reconstruction ran (*iterations, may
+ * be NULL): iters, or fewer when its error target was met. */
+int ptx_server_poll_ex(void* server, long long id, int* done, double* final_loss, double* latency_s,
+                       int* iterations, float* object_out, float* aux_out);
 /* Cancel queued requests, finish the active ones, stop the scheduler and free the server. */
 int ptx_server_destroy(void* server);
 

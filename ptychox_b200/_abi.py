@@ -81,6 +81,7 @@ SIGNATURES: dict[str, tuple] = {
     "ptx_server_create": (_i, [_i, _sz, _i, _p]),
     "ptx_server_submit": (_i, [_p, _p, _p]),
     "ptx_server_poll": (_i, [_p, C.c_longlong, _p, _p, _p, _p, _p]),
+    "ptx_server_poll_ex": (_i, [_p, C.c_longlong, _p, _p, _p, _p, _p, _p]),
     "ptx_server_destroy": (_i, [_p]),
 }
 

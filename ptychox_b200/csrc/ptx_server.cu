@@ -10,10 +10,18 @@
 // stream-ordered pool (kept mapped between reconstructions).  One iteration
 // (fused sweep + one Adam step of each parameter) is captured once per reconstruction as a
 // CUDA graph, with the persistent passes bounded to 8 units per CTA at capture so the
-// kernels of concurrent reconstructions interleave CTA by CTA; a scheduler thread replays
-// the next iteration of every active reconstruction on its own stream (older
-// reconstructions on higher-priority streams, at most two iterations queued per stream)
-// and, when one finishes, reads back its parameters and final loss and frees its memory.
+// kernels of concurrent reconstructions interleave CTA by CTA.  Two threads share the work:
+//   - the scheduler thread only replays: each tick it queues the next iteration of every
+//     active reconstruction on that reconstruction's stream (older reconstructions on
+//     higher-priority streams, at most two iterations queued per stream) and polls events,
+//     so it never waits on the device;
+//   - the admission thread does everything that blocks: it admits queued requests first
+//     come first served within the budget and slot count (allocation, upload, a warm-up
+//     sweep that also gives the initial loss, capture, instantiation) and hands the ready
+//     reconstruction to the scheduler, and it reads back and frees finished ones.
+// A request may stop early at a fixed error: once the loss of a completed iteration falls
+// to target_ratio times the initial loss, no further iteration is queued (the iterations
+// already queued still run).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -50,6 +58,7 @@ struct Request {
   Clock::time_point submitted, finished;
   int status = 0;  // 0 queued, 1 active, 2 done, < 0: -(error code)
   double final_loss = NAN;
+  int iterations = 0;  // iterations run (fewer than d.iters when the error target was met)
   std::vector<unsigned char> obj_out, aux_out;
 };
 
@@ -65,6 +74,9 @@ struct Slot {
   double* loss = nullptr;
   cudaGraphExec_t exec = nullptr;
   int launched = 0;
+  int limit = 0;                // iterations to queue (d.iters, or fewer once the target is met)
+  double target = -1.0;         // stop once a completed iteration's loss is <= target
+  double* loss_host = nullptr;  // page-locked: each replay copies its sweep loss here
   std::deque<cudaEvent_t> inflight;
   std::vector<cudaEvent_t> spare;
   cudaEvent_t done = nullptr;
@@ -83,7 +95,13 @@ struct Server {
   std::map<long long, std::unique_ptr<Request>> requests;
   long long next_id = 1;
   bool stop = false;
-  std::thread worker;
+  // hand-over between the threads (under mu): reconstructions ready to run, finished ones
+  // to read back, the slots and bytes held by admitted (or admitting) reconstructions
+  std::deque<Slot> ready, finished;
+  int slots_held = 0;
+  size_t used = 0;
+  bool scheduler_done = false;
+  std::thread scheduler, admitter;
 };
 
 size_t obj_elems(const ptx_recon_request& d) { return (size_t)d.obj_h * d.obj_w; }
@@ -154,6 +172,7 @@ int run_iteration(const Slot& s) {
 
 void release(Slot& s) {
   if (s.stream) cudaStreamSynchronize(s.stream);
+  if (s.loss_host) cudaFreeHost(s.loss_host);
   for (cudaEvent_t e : s.inflight) cudaEventDestroy(e);
   for (cudaEvent_t e : s.spare) cudaEventDestroy(e);
   s.inflight.clear();
@@ -213,9 +232,18 @@ int admit(Slot& s, Request* r, int priority, cudaMemPool_t pool) {
   // Adam moments (contiguous m_obj .. v_aux), their states and the loss start at zero
   cudaMemsetAsync(s.m_obj, 0, 2 * po + 2 * pa + 3 * 256, st);
   if (cudaGetLastError() != cudaSuccess) return cuda_status(cudaGetLastError(), "server upload");
-  // one sweep outside the capture builds the FFT plans and kernel attributes
+  if (cudaMallocHost(&s.loss_host, sizeof(double)) != cudaSuccess) {
+    return cuda_status(cudaGetLastError(), "server host loss");
+  }
+  *s.loss_host = NAN;
+  // one sweep outside the capture builds the FFT plans and kernel attributes; at the initial
+  // parameters it is also the first iteration's sweep, whose loss sets the error target
   if (int e = run_sweep(s)) return e;
+  double loss0 = NAN;
+  cudaMemcpyAsync(&loss0, s.loss, sizeof(double), cudaMemcpyDeviceToHost, st);
   if (cudaStreamSynchronize(st) != cudaSuccess) return cuda_status(cudaGetLastError(), "server warm-up");
+  s.limit = d.iters;
+  s.target = d.target_ratio > 0.f ? (double)d.target_ratio * loss0 : -1.0;
   // the bound applies to this (scheduler) thread's launches only: another server's
   // scheduler, or the host program's own sweeps, keep theirs
   const int saved_units = set_thread_units_per_cta(kServerUnitsPerCta);
@@ -223,6 +251,10 @@ int admit(Slot& s, Request* r, int priority, cudaMemPool_t pool) {
   int status = cuda_status(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "server capture");
   if (!status) {
     status = run_iteration(s);
+    if (!status && s.target >= 0.0) {
+      status = cuda_status(cudaMemcpyAsync(s.loss_host, s.loss, sizeof(double), cudaMemcpyDeviceToHost, st),
+                           "server loss copy");
+    }
     const cudaError_t end = cudaStreamEndCapture(st, &graph);
     if (!status && end != cudaSuccess) status = cuda_status(end, "server capture end");
   }
@@ -238,14 +270,26 @@ int admit(Slot& s, Request* r, int priority, cudaMemPool_t pool) {
   return PTX_OK;
 }
 
-// Queue the next iteration unless kServerMaxInflight are still queued; true if launched.
+// Queue the next iteration unless kServerMaxInflight are still queued or the schedule is
+// complete; true if launched.  With an error target, a completed iteration whose loss (copied
+// to loss_host by the replay) is at or below it ends the schedule: the iterations already
+// queued run and `done` is recorded behind them.
 bool launch_next(Slot& s, int* err) {
+  bool completed = false;
   while (!s.inflight.empty() && cudaEventQuery(s.inflight.front()) == cudaSuccess) {
     s.spare.push_back(s.inflight.front());
     s.inflight.pop_front();
+    completed = true;
   }
   cudaGetLastError();
-  if (s.launched >= s.req->d.iters || (int)s.inflight.size() >= kServerMaxInflight) return false;
+  if (completed && s.target >= 0.0 && s.launched < s.limit) {
+    const double seen = *static_cast<volatile double*>(s.loss_host);
+    if (seen <= s.target) {
+      s.limit = s.launched;
+      cudaEventRecord(s.done, s.stream);
+    }
+  }
+  if (s.launched >= s.limit || (int)s.inflight.size() >= kServerMaxInflight) return false;
   if (cudaGraphLaunch(s.exec, s.stream) != cudaSuccess) {
     *err = cuda_status(cudaGetLastError(), "server graph launch");
     return false;
@@ -260,7 +304,7 @@ bool launch_next(Slot& s, int* err) {
   }
   cudaEventRecord(ev, s.stream);
   s.inflight.push_back(ev);
-  if (++s.launched == s.req->d.iters) cudaEventRecord(s.done, s.stream);
+  if (++s.launched == s.limit) cudaEventRecord(s.done, s.stream);
   return true;
 }
 
@@ -275,45 +319,24 @@ int collect(Slot& s) {
   cudaMemcpyAsync(&loss, s.loss, sizeof(double), cudaMemcpyDeviceToHost, s.stream);
   if (cudaStreamSynchronize(s.stream) != cudaSuccess) return cuda_status(cudaGetLastError(), "server read-back");
   r->final_loss = loss;
+  r->iterations = s.launched;
   return PTX_OK;
 }
 
-void serve(Server* sv) {
+// Scheduler thread: replays only.  Takes ready reconstructions, queues one iteration per
+// active reconstruction per tick, and passes finished (or failed) ones to the admission
+// thread; it never synchronises with the device.
+void schedule(Server* sv) {
   cudaSetDevice(sv->device);
-  int least = 0, greatest = 0;
-  cudaDeviceGetStreamPriorityRange(&least, &greatest);
   std::vector<Slot> active;
-  size_t used = 0;
   for (;;) {
-    // admission: first come first served, within the budget and the slot count
-    for (;;) {
-      Request* r = nullptr;
-      {
-        std::unique_lock<std::mutex> lock(sv->mu);
-        if (sv->stop) {
-          for (Request* q : sv->queued) q->status = -PTX_ERR_INVALID_ARGUMENT;  // cancelled
-          sv->queued.clear();
-        }
-        if (sv->queued.empty() || (int)active.size() >= sv->max_active) break;
-        r = sv->queued.front();
-        if (used + r->bytes > sv->budget && !active.empty()) break;
-        sv->queued.pop_front();
-        r->status = 1;
+    {
+      std::lock_guard<std::mutex> lock(sv->mu);
+      while (!sv->ready.empty()) {
+        active.push_back(sv->ready.front());
+        sv->ready.pop_front();
       }
-      Slot s;
-      const int prio = std::max(greatest, std::min(least, greatest + (int)active.size()));
-      const int e = admit(s, r, prio, sv->pool);
-      if (e) {
-        release(s);
-        std::lock_guard<std::mutex> lock(sv->mu);
-        r->status = -e;
-        r->finished = Clock::now();
-        continue;
-      }
-      used += r->bytes;
-      active.push_back(s);
     }
-    // one iteration per active reconstruction per tick
     bool progressed = false;
     for (Slot& s : active) {
       int err = 0;
@@ -323,36 +346,119 @@ void serve(Server* sv) {
         s.req->status = -err;
       }
     }
-    // retire finished (or failed) reconstructions
     for (size_t i = 0; i < active.size();) {
       Slot& s = active[i];
-      const bool failed = s.req->status < 0;
-      if (!failed && !(s.launched == s.req->d.iters && cudaEventQuery(s.done) == cudaSuccess)) {
+      bool failed;
+      {
+        std::lock_guard<std::mutex> lock(sv->mu);
+        failed = s.req->status < 0;
+      }
+      if (!failed && !(s.launched == s.limit && cudaEventQuery(s.done) == cudaSuccess)) {
         cudaGetLastError();
         ++i;
         continue;
       }
-      const int e = failed ? 0 : collect(s);
-      Request* r = s.req;
-      used -= r->bytes;
-      release(s);
       {
         std::lock_guard<std::mutex> lock(sv->mu);
-        r->status = failed ? r->status : (e ? -e : 2);
-        r->finished = Clock::now();
+        sv->finished.push_back(s);
       }
       sv->cv.notify_all();
       active.erase(active.begin() + i);
       progressed = true;
     }
     std::unique_lock<std::mutex> lock(sv->mu);
-    if (sv->stop && sv->queued.empty() && active.empty()) break;
-    if (active.empty() && sv->queued.empty()) {
+    if (sv->stop && sv->queued.empty() && sv->ready.empty() && active.empty() && sv->slots_held == 0) break;
+    if (active.empty() && sv->ready.empty()) {
       sv->cv.wait_for(lock, std::chrono::milliseconds(5));
     } else if (!progressed) {
       lock.unlock();
       std::this_thread::sleep_for(std::chrono::microseconds(20));
     }
+  }
+  std::lock_guard<std::mutex> lock(sv->mu);
+  sv->scheduler_done = true;
+  sv->cv.notify_all();
+}
+
+// Admission thread: everything that waits on the device.  Reads back and frees finished
+// reconstructions (returning their bytes and slot), then admits queued requests first come
+// first served within the budget and slot count, one at a time, and hands each ready
+// reconstruction to the scheduler.
+void admit_loop(Server* sv) {
+  cudaSetDevice(sv->device);
+  int least = 0, greatest = 0;
+  cudaDeviceGetStreamPriorityRange(&least, &greatest);
+  for (;;) {
+    Slot done_slot;
+    bool have_done = false;
+    Request* r = nullptr;
+    int prio = greatest;
+    {
+      std::unique_lock<std::mutex> lock(sv->mu);
+      for (;;) {
+        if (sv->stop) {
+          for (Request* q : sv->queued) {
+            q->status = -PTX_ERR_INVALID_ARGUMENT;  // cancelled
+            q->finished = Clock::now();
+          }
+          sv->queued.clear();
+        }
+        if (!sv->finished.empty()) {
+          done_slot = sv->finished.front();
+          sv->finished.pop_front();
+          have_done = true;
+          break;
+        }
+        if (!sv->queued.empty() && sv->slots_held < sv->max_active &&
+            (sv->used + sv->queued.front()->bytes <= sv->budget || sv->slots_held == 0)) {
+          r = sv->queued.front();
+          sv->queued.pop_front();
+          r->status = 1;
+          sv->used += r->bytes;
+          prio = std::max(greatest, std::min(least, greatest + sv->slots_held));
+          ++sv->slots_held;
+          break;
+        }
+        if (sv->scheduler_done) return;
+        sv->cv.wait_for(lock, std::chrono::milliseconds(5));
+      }
+    }
+    if (have_done) {
+      Request* q = done_slot.req;
+      bool failed;
+      {
+        std::lock_guard<std::mutex> lock(sv->mu);
+        failed = q->status < 0;
+      }
+      const int e = failed ? 0 : collect(done_slot);
+      release(done_slot);
+      {
+        std::lock_guard<std::mutex> lock(sv->mu);
+        q->status = failed ? q->status : (e ? -e : 2);
+        q->finished = Clock::now();
+        sv->used -= q->bytes;
+        --sv->slots_held;
+      }
+      sv->cv.notify_all();
+      continue;
+    }
+    Slot s;
+    const int e = admit(s, r, prio, sv->pool);
+    if (e) {
+      release(s);
+      std::lock_guard<std::mutex> lock(sv->mu);
+      r->status = -e;
+      r->finished = Clock::now();
+      sv->used -= r->bytes;
+      --sv->slots_held;
+      sv->cv.notify_all();
+      continue;
+    }
+    {
+      std::lock_guard<std::mutex> lock(sv->mu);
+      sv->ready.push_back(s);
+    }
+    sv->cv.notify_all();
   }
 }
 
@@ -376,6 +482,7 @@ int validate(const ptx_recon_request& d) {
       return set_error(PTX_ERR_INVALID_ARGUMENT, "missing transfer function");
     }
   }
+  if (!(d.target_ratio >= 0.f)) return set_error(PTX_ERR_INVALID_ARGUMENT, "target_ratio must be >= 0");
   for (int c : {d.constrain_obj, d.constrain_aux}) {
     if (c < PTX_CONSTRAIN_NONE || c > PTX_CONSTRAIN_REAL_NONNEGATIVE) {
       return set_error(PTX_ERR_INVALID_ARGUMENT, "unknown constraint %d", c);
@@ -429,7 +536,8 @@ int ptx_server_create(int device, size_t hbm_budget, int max_active, void** serv
   }
   unsigned long long keep = ~0ull;
   cudaMemPoolSetAttribute(sv->pool, cudaMemPoolAttrReleaseThreshold, &keep);
-  sv->worker = std::thread(serve, sv);
+  sv->scheduler = std::thread(schedule, sv);
+  sv->admitter = std::thread(admit_loop, sv);
   *server = sv;
   return PTX_OK;
 }
@@ -485,6 +593,11 @@ int ptx_server_submit(void* server, const ptx_recon_request* request, long long*
 
 int ptx_server_poll(void* server, long long id, int* done, double* final_loss, double* latency_s, float* object_out,
                     float* aux_out) {
+  return ptx_server_poll_ex(server, id, done, final_loss, latency_s, nullptr, object_out, aux_out);
+}
+
+int ptx_server_poll_ex(void* server, long long id, int* done, double* final_loss, double* latency_s, int* iterations,
+                       float* object_out, float* aux_out) {
   if (!server || !done) return set_error(PTX_ERR_INVALID_ARGUMENT, "null pointer argument");
   auto* sv = static_cast<Server*>(server);
   std::lock_guard<std::mutex> lock(sv->mu);
@@ -501,6 +614,7 @@ int ptx_server_poll(void* server, long long id, int* done, double* final_loss, d
   *done = 1;
   if (final_loss) *final_loss = r.final_loss;
   if (latency_s) *latency_s = std::chrono::duration<double>(r.finished - r.submitted).count();
+  if (iterations) *iterations = r.iterations;
   if (object_out) std::memcpy(object_out, r.obj_out.data(), r.obj_out.size());
   if (aux_out) std::memcpy(aux_out, r.aux_out.data(), r.aux_out.size());
   sv->requests.erase(it);
@@ -515,7 +629,8 @@ int ptx_server_destroy(void* server) {
     sv->stop = true;
   }
   sv->cv.notify_all();
-  if (sv->worker.joinable()) sv->worker.join();
+  if (sv->scheduler.joinable()) sv->scheduler.join();
+  if (sv->admitter.joinable()) sv->admitter.join();
   if (sv->pool) cudaMemPoolDestroy(sv->pool);
   delete sv;
   return PTX_OK;

@@ -35,7 +35,7 @@ class PtxReconRequest(C.Structure):
         ("batch", C.c_int), ("downsample", C.c_int), ("iters", C.c_int), ("scale", C.c_float),
         ("lr_obj", C.c_float), ("lr_aux", C.c_float), ("constrain_obj", C.c_int), ("constrain_aux", C.c_int),
         ("obj0", C.c_void_p), ("aux0", C.c_void_p), ("scan", C.c_void_p), ("measured", C.c_void_p),
-        ("transfer_1", C.c_void_p), ("transfer_2", C.c_void_p),
+        ("transfer_1", C.c_void_p), ("transfer_2", C.c_void_p), ("target_ratio", C.c_float),
     ]
 
 
@@ -67,7 +67,8 @@ class NativeReconstructionServer:
             scale=float(req.scale), lr_obj=float(req.lrs[0]), lr_aux=float(req.lrs[1]),
             constrain_obj=CONSTRAINTS[req.constraints[0]], constrain_aux=CONSTRAINTS[req.constraints[1]],
             obj0=obj.ctypes.data, aux0=aux.ctypes.data, scan=scan.ctypes.data, measured=meas.ctypes.data,
-            transfer_1=None if t1 is None else t1.ctypes.data, transfer_2=None if t2 is None else t2.ctypes.data)
+            transfer_1=None if t1 is None else t1.ctypes.data, transfer_2=None if t2 is None else t2.ctypes.data,
+            target_ratio=float(req.target_ratio or 0.0))
         rid = C.c_longlong(0)
         _abi.call("ptx_server_submit", self._h, C.addressof(d), C.addressof(rid))
         self._shapes[rid.value] = (req, obj.shape, aux.shape)
@@ -81,10 +82,10 @@ class NativeReconstructionServer:
         req, so, sa = self._shapes[rid]
         obj = np.empty(so, np.complex64)
         aux = np.empty(sa, np.complex64)
-        done, loss, lat = C.c_int(0), C.c_double(0.0), C.c_double(0.0)
+        done, loss, lat, iters = C.c_int(0), C.c_double(0.0), C.c_double(0.0), C.c_int(0)
         try:
-            _abi.call("ptx_server_poll", self._h, C.c_longlong(rid), C.addressof(done), C.addressof(loss),
-                      C.addressof(lat), obj.ctypes.data, aux.ctypes.data)
+            _abi.call("ptx_server_poll_ex", self._h, C.c_longlong(rid), C.addressof(done), C.addressof(loss),
+                      C.addressof(lat), C.addressof(iters), obj.ctypes.data, aux.ctypes.data)
         except Exception:
             del self._shapes[rid]
             raise
@@ -92,7 +93,7 @@ class NativeReconstructionServer:
             return None
         del self._shapes[rid]
         return ReconResult(req.rid, req.modality, req.arrival, admitted=0.0, finished=req.arrival + lat.value,
-                           final_loss=loss.value, obj=obj, aux=aux, sweeps=int(req.iters))
+                           final_loss=loss.value, obj=obj, aux=aux, sweeps=int(iters.value))
 
     def run(self, requests: list[ReconRequest], poll_interval: float = 1e-3) -> list[ReconResult]:
         """Submit all ``requests`` now and wait for them; results in ``rid`` order."""

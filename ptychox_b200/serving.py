@@ -10,6 +10,9 @@ Reconstructions of mixed modality and size arrive over time.  The server
 * every scheduler tick replays the next iteration of every active reconstruction on its
   own stream, so iterations of different reconstructions overlap on the device, and
   reconstructions join as soon as earlier ones finish and free their memory;
+* stops a reconstruction at a fixed error when its request asks for one: each replay copies
+  its sweep loss to page-locked memory, and once a completed iteration's loss is at most
+  ``target_ratio`` times the initial loss no further iteration is queued;
 * reports per-request latency (arrival to final state on the host), p50 / p99, and
   sweeps/s.
 
@@ -61,6 +64,9 @@ class ReconRequest:
     t1: np.ndarray | None = None
     t2: np.ndarray | None = None
     ds: int = 1
+    # stop at a fixed error: once an iteration's loss is at most target_ratio times the initial
+    # loss (the sweep at obj0 / aux0) no further iteration runs; 0 runs all `iters`
+    target_ratio: float = 0.0
 
     def units(self) -> int:
         return int(self.pos.shape[0])
@@ -142,10 +148,15 @@ class _Slot:
             self.adam = FusedAdam([self.obj, self.aux], list(req.lrs), constraints=list(req.constraints))
         self.stream_handle = self.stream.cuda_stream
         self.graph = None
+        self.limit = req.iters  # iterations to run (fewer once the error target is met)
+        self.loss_host = torch.full((), float("nan"), dtype=torch.float64).pin_memory()
+        # the warm-up sweep (FFT plans and kernel attributes, outside any capture) runs at
+        # obj0 / aux0: its loss is the initial loss the error target is relative to
+        with torch.cuda.stream(self.stream):
+            self._sweep()
+        self.stream.synchronize()
+        self.target = float(req.target_ratio) * float(self.loss.item()) if req.target_ratio > 0 else -1.0
         if use_graph:
-            with torch.cuda.stream(self.stream):
-                self._sweep()  # builds FFT plans and kernel attributes outside the capture
-            self.stream.synchronize()
             self.graph = torch.cuda.CUDAGraph()
             with torch.cuda.stream(self.stream):
                 self.graph.capture_begin(capture_error_mode="relaxed")
@@ -178,12 +189,21 @@ class _Slot:
     def _iterate(self) -> None:
         self._sweep()
         self.adam.step([self.g_obj, self.g_aux])
+        if self.target >= 0.0:
+            self.loss_host.copy_(self.loss, non_blocking=True)
 
     def launch_next(self, max_inflight: int) -> None:
-        """Queue the next iteration unless ``max_inflight`` of this slot's are still queued."""
+        """Queue the next iteration unless ``max_inflight`` of this slot's are still queued, the
+        schedule is complete, or a completed iteration met the error target."""
+        completed = False
         while self.inflight and self.inflight[0].query():
             self.inflight.pop(0)
-        if self.iters_launched >= self.req.iters or len(self.inflight) >= max_inflight:
+            completed = True
+        if completed and self.target >= 0.0 and self.iters_launched < self.limit:
+            if float(self.loss_host) <= self.target:
+                self.limit = self.iters_launched
+                self.done.record(self.stream)
+        if self.iters_launched >= self.limit or len(self.inflight) >= max_inflight:
             return
         with torch.cuda.stream(self.stream):
             if self.graph is not None:
@@ -194,11 +214,11 @@ class _Slot:
         ev = torch.cuda.Event()
         ev.record(self.stream)
         self.inflight.append(ev)
-        if self.iters_launched == self.req.iters:
+        if self.iters_launched == self.limit:
             self.done.record(self.stream)
 
     def finished(self) -> bool:
-        return self.iters_launched == self.req.iters and self.done.query()
+        return self.iters_launched == self.limit and self.done.query()
 
 
 class ReconstructionServer:
@@ -266,7 +286,7 @@ class ReconstructionServer:
                     res.final_loss = float(slot.loss.item())
                     res.obj = slot.obj.cpu().numpy()
                     res.aux = slot.aux.cpu().numpy()
-                    res.sweeps = slot.req.iters
+                    res.sweeps = slot.iters_launched
                     res.finished = clock() if realtime else 0.0
                     used -= slot.bytes
                     slot.graph = None
@@ -305,7 +325,9 @@ def run_plain(requests: list[ReconRequest], device: torch.device | str = "cuda",
         opt = torch.optim.Adam([{"params": [obj], "lr": req.lrs[0]}, {"params": [aux], "lr": req.lrs[1]}],
                                betas=(0.9, 0.999), eps=1e-16)
         loss = None
-        for _ in range(req.iters):
+        target = -1.0
+        done_iters = 0
+        for it in range(req.iters):
             if req.modality == "conventional":
                 pred = ptychoX_base(obj, aux, pos)
             elif req.modality == "fourier":
@@ -318,6 +340,7 @@ def run_plain(requests: list[ReconRequest], device: torch.device | str = "cuda",
             opt.zero_grad(set_to_none=True)
             loss.backward()
             opt.step()
+            done_iters = it + 1
             with torch.no_grad():
                 for p, c in ((obj, req.constraints[0]), (aux, req.constraints[1])):
                     if c == "unit_amplitude":
@@ -325,10 +348,16 @@ def run_plain(requests: list[ReconRequest], device: torch.device | str = "cuda",
                         p.copy_(torch.where(a > 1, p / a.clamp_min(1e-30), p))
                     elif c == "real_nonnegative":
                         p.copy_(p.real.clamp_min(0.0).to(torch.complex64))
+            if req.target_ratio > 0:  # the reference loop reads every loss (train_ptychography.py:560)
+                value = float(loss.item())
+                if it == 0:
+                    target = float(req.target_ratio) * value
+                if value <= target:
+                    break
         res.final_loss = float(loss.item())
         res.obj = obj.detach().cpu().numpy()
         res.aux = aux.detach().cpu().numpy()
-        res.sweeps = req.iters
+        res.sweeps = done_iters
         res.finished = time.perf_counter() - t0
         out.append(res)
     return sorted(out, key=lambda r: r.rid)
@@ -353,7 +382,7 @@ def snap_pow2(n: float) -> int:
 
 
 def synthesize_request(rid: int, modality: str, arrival: float, size: dict, seed: int, device,
-                       iters: int = 50) -> ReconRequest:
+                       iters: int = 50, target_ratio: float = 0.0) -> ReconRequest:
     """One seeded reconstruction problem; counts from the forward model of the truth.
 
     ``size``: conventional {"p", "grid", "step", "n"}; fourier {"n", "h", "grid"};
@@ -410,7 +439,7 @@ def synthesize_request(rid: int, modality: str, arrival: float, size: dict, seed
     aux0 = (aux_true * np.exp(0.05j * rng.standard_normal(aux_true.shape))).astype(np.complex64)
     return ReconRequest(rid=rid, modality=modality, arrival=float(arrival), obj0=obj0, aux0=aux0, pos=pos,
                         meas=counts.cpu().numpy(), scale=scale, iters=iters, lrs=lrs, constraints=cons, t1=t1,
-                        t2=t2, ds=ds)
+                        t2=t2, ds=ds, target_ratio=float(target_ratio))
 
 
 def serving_mix(n_requests: int, seed: int = 0, rate: float = 20.0) -> list[tuple]:
@@ -419,11 +448,12 @@ def serving_mix(n_requests: int, seed: int = 0, rate: float = 20.0) -> list[tupl
     Poisson arrivals at ``rate`` per second; 40 / 30 / 20 / 10 % drawn from the
     conventional small scan (128^2 probe, 11x11 raster), Fourier (256^2 pupil, 15x15
     LEDs, 1024^2 spectrum), coded / near-field (1024^2 field, 64 shifts, ds 4) and the
-    conventional large scan (512^2 probe, 30x30 raster); sizes jittered by U[0.75, 1.25]
-    and snapped to the lengths of the register-FFT kernels: probe sides to the nearest
-    power of two (other 2^a 3^b 5^c lengths run on the slower runtime-plan kernels), scan
-    grids jittered with positions capped at 900 and floored at 49, Fourier and coded sides
-    kept (powers of two).
+    conventional large scan (512^2 probe, 30x30 raster), sizes jittered by U[0.75, 1.25]:
+    conventional probe sides snapped to the nearest 2^a 3^b 5^c length (96..640: lengths
+    such as 100, 120, 144, 160, 480, 600 run on the runtime-plan FFT kernels), scan grids
+    jittered with positions held in [49, 900], Fourier LED grids and coded shift counts
+    jittered; the Fourier and coded sides stay powers of two (their kernels are the
+    power-of-two register FFT, and 1024 / 256 are the only powers of two within 25%).
     """
     rng = np.random.default_rng(seed)
     t = 0.0
@@ -435,7 +465,7 @@ def serving_mix(n_requests: int, seed: int = 0, rate: float = 20.0) -> list[tupl
         if u < 0.4 or u >= 0.9:
             big = u >= 0.9
             p0, g0, s0 = (512, 30, 48) if big else (128, 11, 32)
-            p = snap_pow2(p0 * j())
+            p = snap_smooth(p0 * j())
             grid = int(min(30, max(7, round(g0 * j()))))
             step = max(4, int(round(s0 * p / p0)))
             n = 8 + (grid - 1) * step + p + 4 + 8

@@ -92,3 +92,34 @@ def test_replicas_spread_requests_and_match():
         assert g.rid == w.rid
         assert abs(g.final_loss - w.final_loss) <= 1e-4 * abs(w.final_loss)
         assert rel_l2(g.obj, w.obj) < 1e-4
+
+
+def test_stop_at_fixed_error_in_every_server():
+    """A request with a target ratio stops once a completed iteration's loss is at most that
+    fraction of its initial loss, in the Python server, the native server and the plain loop;
+    the servers may run the iterations already queued (at most two) beyond the one that met it.
+    The ratio is the plain loop's own loss ratio after six iterations, so the target is met."""
+    import copy
+
+    from ptychox_b200.native_server import NativeReconstructionServer
+    from ptychox_b200.serving import ReconstructionServer, run_plain
+
+    reqs = []
+    for r in small_mix()[:4]:
+        r1, r6 = copy.copy(r), copy.copy(r)
+        r1.iters, r6.iters = 1, 6
+        l0 = run_plain([r1], "cuda", realtime=False)[0].final_loss
+        l6 = run_plain([r6], "cuda", realtime=False)[0].final_loss
+        if l6 < 0.99 * l0:
+            r.iters, r.target_ratio = 40, float(l6 / l0) * (1 + 1e-6)
+            reqs.append(r)
+    assert reqs, "no request lowered its loss in six iterations"
+    plain = run_plain(reqs, "cuda", realtime=False)
+    served = ReconstructionServer("cuda", max_active=8).run(reqs, realtime=False)
+    with NativeReconstructionServer(0, max_active=8) as srv:
+        native = srv.run(reqs)
+    for p, s, n in zip(plain, served, native):
+        assert 1 <= p.sweeps <= 6
+        for other in (s, n):
+            assert p.sweeps - 1 <= other.sweeps <= p.sweeps + 3
+            assert np.isfinite(other.final_loss)
