@@ -143,6 +143,63 @@ class Conventional(Workload):
         O.base_sweep(h["obj"], h["aux"], h["pos"][:k], meas[:k], scale, fp64=False, workers=workers)
 
 
+class ConventionalSubpixel(Conventional):
+    """Conventional ptychography at sub-pixel scan positions: config 1's raster with its
+    U[-3, 3] jitter kept real (float64 positions), the five-pass sub-pixel sweep."""
+
+    def metric(self):
+        return f"fwd+adj sweeps/s ({self.batch}×{self.p}²→{self.n_obj}², sub-pixel positions)"
+
+    def config(self):
+        c = super().config()
+        c["modality"] = "conventional, sub-pixel positions (Fourier-shifted windows)"
+        c["raster"] = c["raster"] + " (real-valued)"
+        return c
+
+    def host(self, seed):
+        from ptychox_b200 import synth
+
+        rng = np.random.default_rng(seed)
+        obj = synth.random_object(self.n_obj, self.n_obj, rng)
+        probe = synth.gaussian_probe(self.p, self.p, rng)
+        pos = synth.raster_positions_subpixel(self.grid, self.step, self.origin, float(self.jitter), rng)
+        guess = (obj * (1 + 0.1 * rng.standard_normal(obj.shape))).astype(np.complex64)
+        return {"truth": obj, "obj": guess, "aux": probe, "pos": pos}
+
+    def synth(self, seed, dev):
+        import torch
+
+        from ptychox_b200 import ptychoX_base_subpixel
+
+        h = self.host(seed)
+        with torch.no_grad():
+            amp = ptychoX_base_subpixel(torch.from_numpy(h["truth"]).to(dev), torch.from_numpy(h["aux"]).to(dev),
+                                        torch.from_numpy(h["pos"]).to(dev))
+            meas, scale = device_poisson(amp, self.photons, seed, per_pixel=False)
+        return self._pack(h, meas, scale, dev)
+
+    def workspace(self, prob, dev):
+        from ptychox_b200 import _abi
+        from ptychox_b200._utils import workspace
+
+        return workspace(_abi.query("ptx_base_subpix_workspace_bytes", self.p, self.p, self.batch), dev)
+
+    def sweep(self, prob, ws):
+        from ptychox_b200.base import base_subpixel_sweep
+
+        return base_subpixel_sweep(prob["obj"], prob["aux"], prob["pos"], prob["meas"], prob["scale"], ws=ws)
+
+    def loss_api(self, obj, aux, pos, prob):
+        from ptychox_b200 import ptychoX_base_subpixel_loss
+
+        return ptychoX_base_subpixel_loss(obj, aux, pos, prob["meas"], prob["scale"])
+
+    def cpu_sweep(self, h, meas, scale, k, workers):
+        from oracle import ptycho_oracle as O
+
+        O.base_subpix_sweep(h["obj"], h["aux"], h["pos"][:k], meas[:k], scale, fp64=False, workers=workers)
+
+
 class Fourier(Conventional):
     """Fourier ptychography (config 2): 15x15 LEDs, 256^2 pupil, 1024^2 spectrum."""
 
@@ -299,6 +356,7 @@ WORKLOADS = {
     for w in [
         Conventional("conventional-900x512-2048", 2048, 512, 30, 48, 64, 3, 1e5),
         Conventional("conventional-121x128-512", 512, 128, 11, 32, 8, 2, 1e4),
+        ConventionalSubpixel("conventional-subpixel-900x512-2048", 2048, 512, 30, 48, 64, 3, 1e5),
         Fourier("fourier-225x256-1024", 1024, 256, 15, 5e3),
         Coded("coded-64x1024-ds4", 1024, 64, 4, 2e3, nearfield=False),
         Coded("nearfield-64x1024-ds4", 1024, 64, 4, 2e3, nearfield=True),
@@ -602,6 +660,12 @@ def run_ours(args) -> None:
         cpu_port = cpu_sample_rate(wl, host, meas_host, prob["scale"], budget_s=args.cpu_budget / 2)
         if cpu is None:
             cpu, cpu_port = cpu_port, None
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_reference_gpu:
+        ref_gpu = reference_gpu_rates(wl, host, prob["meas"].cpu().numpy(), prob["scale"], dev, flush)
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serving and not args.units and wl.name == DEFAULT_WORKLOAD:
+        serving = serving_record(args, dev)
 
     if rank == 0:
         cfg = wl.config()
@@ -624,6 +688,8 @@ def run_ours(args) -> None:
             "roofline": roofline,
             "cpu_baseline": cpu,
             "cpu_baseline_port": cpu_port,
+            "reference_gpu": ref_gpu,
+            "serving": serving,
             "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clk,
@@ -693,6 +759,8 @@ def reference_sweep_fn(wl, ref, h, meas, scale, device="cpu", use_cuda_kernels=F
 
         def forward():
             return ref.ptychoX_fourier(obj, aux, led, use_cuda_kernels=use_cuda_kernels)
+    elif isinstance(wl, ConventionalSubpixel):
+        forward = reference_subpixel_forward(ref, obj, aux, h["pos"], use_cuda_kernels)
     else:
         pos = torch.from_numpy(np.asarray(h["pos"], dtype=np.int64)).to(dev)
 
@@ -707,6 +775,32 @@ def reference_sweep_fn(wl, ref, h, meas, scale, device="cpu", use_cuda_kernels=F
         return loss.detach()
 
     return one
+
+
+def reference_subpixel_forward(ref, obj, probe, positions, use_cuda_kernels=False):
+    """The sub-pixel operator composed from the reference's own functions (it has none of its
+    own): the window at floor(p + 1/2) cropped as base/ops.py:61-62 does, shifted by the
+    fraction with shift_phase_ramp (coded/ops.py:157-171) on its spectrum, then ptychoX_base on
+    the shifted patches.  Returns a callable giving the amplitudes."""
+    import torch
+    from ptychoX.coded.ops import shift_phase_ramp
+
+    ph, pw = probe.shape
+    pos = np.asarray(positions, dtype=np.float64)
+    corner = np.floor(pos + 0.5)
+    frac = pos - corner
+    shifts = torch.from_numpy(np.stack([frac[:, 0] / pw, frac[:, 1] / ph], axis=1)).to(obj.device, obj.real.dtype)
+    corners = corner.astype(np.int64).tolist()
+    zero = torch.zeros(1, 2, dtype=torch.long, device=obj.device)
+
+    def forward():
+        ramp = shift_phase_ramp(ph, pw, shifts, obj.device, obj.real.dtype)
+        crops = torch.stack([obj[y : y + ph, x : x + pw] for x, y in corners])
+        patches = torch.fft.ifft2(torch.fft.fft2(crops) * ramp)
+        return torch.cat([ref.ptychoX_base(patches[b], probe, zero, use_cuda_kernels=use_cuda_kernels)
+                          for b in range(len(corners))], dim=0)
+
+    return forward
 
 
 def reference_counts(wl, ref, h, seed=7):
@@ -725,6 +819,8 @@ def reference_counts(wl, ref, h, seed=7):
                                     t(np.asarray(h["pos"], dtype=np.float32)), wl.ds)
         elif isinstance(wl, Fourier):
             amp = ref.ptychoX_fourier(t(h["truth"]), t(h["aux"]), t(np.asarray(h["pos"], dtype=np.int64)))
+        elif isinstance(wl, ConventionalSubpixel):
+            amp = reference_subpixel_forward(ref, t(h["truth"]), t(h["aux"]), h["pos"])()
         else:
             amp = ref.ptychoX_base(t(h["truth"]), t(h["aux"]), t(np.asarray(h["pos"], dtype=np.int64)))
     rng = np.random.default_rng(seed)
@@ -757,8 +853,56 @@ def cpu_reference_rate(wl, host, measured, scale, budget_s: float = 12.0) -> dic
         torch.set_num_threads(prev)
     return {"value": 1.0 / dt, "unit": "sweeps/s", "cores": threads, "kind": "reference",
             "sample": f"{reps} whole sweeps ({wl.batch} {wl.units} each) after one warm-up sweep; the reference's "
-                      f"ptychoX (baseline/_ref) with use_cuda_kernels=False in complex64 + F.mse_loss + backward, "
+                      f"ptychoX (baseline/_ref) with use_cuda_kernels=False in complex64 + F.mse_loss (train_coded's fd_loss for the fd workloads) + backward, "
                       f"torch CPU on {threads} threads ({dt:.2f} s per sweep)"}
+
+
+def reference_gpu_rates(wl, host, measured, scale, dev, flush, steps: int = 5, warmup: int = 2) -> dict | None:
+    """The reference's own GPU paths on this B200, one request at a time: its PyTorch operator on
+    CUDA tensors (torch.fft / cuFFT through ATen, ``use_cuda_kernels=False``) and its pybind11
+    CUDA extension (``python/ptychoX/csrc``, built from source for sm_100a into baseline/_ref,
+    ``use_cuda_kernels=True``), each a whole sweep per step (operator, F.mse_loss, backward)
+    timed with CUDA events, L2 flushed between steps.  None without the reference install."""
+    import importlib
+
+    import torch
+
+    ref = reference_package()
+    if ref is None:
+        return None
+    out = {}
+    for label, use_ext in (("torch_cuda", False), ("csrc_extension", True)):
+        if use_ext and isinstance(wl, ConventionalSubpixel):
+            continue
+        try:
+            one = reference_sweep_fn(wl, ref, host, measured, scale, device=dev, use_cuda_kernels=use_ext)
+            for _ in range(warmup):
+                one()
+            torch.cuda.synchronize(dev)
+            stream = torch.cuda.current_stream(dev)
+            times = []
+            for _ in range(steps):
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                one()
+                b.record(stream)
+                flush.zero_()
+                torch.cuda.synchronize(dev)
+                times.append(a.elapsed_time(b))
+            ms = statistics.median(times)
+            rec = {"value": 1e3 / ms, "unit": "sweeps/s", "ms_per_sweep": ms, "steps": steps}
+            if use_ext:
+                mod = {"Coded": "coded", "Fourier": "fpm"}.get(type(wl).__name__, "base")
+                rec["module"] = str(Path(importlib.import_module(f"ptychoX.{mod}._C").__file__).relative_to(ROOT))
+            out[label] = rec
+        except Exception as e:  # report, do not fail the bench line
+            out[label] = {"error": f"{type(e).__name__}: {e}"[:300]}
+        torch.cuda.empty_cache()
+    out["method"] = ("the reference's ptychoX (baseline/_ref), one whole sweep per step as its training drivers run "
+                     "it: operator with use_cuda_kernels False (torch.fft on CUDA) or True (its cuFFT extension "
+                     "compiled for sm_100a), F.mse_loss, backward; CUDA events, median of steps")
+    return out
 
 
 def cpu_sample_rate(wl, host, measured, scale, budget_s: float = 12.0) -> dict:
@@ -822,7 +966,8 @@ def run_reference(args) -> None:
         per_sweep = statistics.mean(times)
         kind = "reference"
         sample = (f"whole sweeps ({batch} {wl.units} each): the reference's ptychoX from baseline/_ref, "
-                  f"use_cuda_kernels=False, complex64, F.mse_loss + backward, torch CPU on {threads} threads")
+                  f"use_cuda_kernels=False, complex64, F.mse_loss (fd_loss for the fd workloads) + backward, "
+                  f"torch CPU on {threads} threads")
     else:
         from oracle import ptycho_oracle as O
 
@@ -835,6 +980,8 @@ def run_reference(args) -> None:
                                                fp64=False, workers=workers)
             elif isinstance(wl, Fourier):
                 amp, _, _ = O.fpm_forward(h["truth"], h["aux"], h["pos"][:k], fp64=False, workers=workers)
+            elif isinstance(wl, ConventionalSubpixel):
+                amp, _, _ = O.base_subpix_forward(h["truth"], h["aux"], h["pos"][:k], fp64=False, workers=workers)
             else:
                 amp, _, _ = O.base_forward(h["truth"], h["aux"], h["pos"][:k], fp64=False, workers=workers)
             from ptychox_b200 import synth
@@ -915,32 +1062,33 @@ def run_native(reqs, warm, dev, max_active):
     return [out[k] for k in sorted(out)], wall
 
 
-def run_serving(args) -> None:
-    """Served mixed stream vs one-at-a-time plain solves on the same GPU.
+def serving_record(args, dev) -> dict:
+    """Served mixed stream vs one-at-a-time plain solves on the same GPU (config 4).
 
     The stream: ``--requests`` reconstructions (default 40), Poisson arrivals at 20/s,
-    40/30/20/10 % from configs 0/2/3/1 with sizes jittered +-25 %, 50 iterations each.
+    40/30/20/10 % from configs 0/2/3/1 with sizes jittered +-25 %, up to ``--iters`` (50)
+    iterations each, stopping at a fixed error (``--target-ratio`` times the initial loss).
     Requests are synthesised (seeded, counts from the forward model) before the clock
-    starts; their host arrays are uploaded at admission, inside the measured latency.
-    """
+    starts; their host arrays are uploaded at admission, inside the measured latency.  The
+    same requests run through the Python server, the native server (``ptx_server_*``,
+    submitted at their arrival times) and the plain loop (unfused operators,
+    F.mse_loss, torch.optim.Adam, one request at a time)."""
     import torch
 
     from ptychox_b200 import _abi
     from ptychox_b200.serving import (ReconstructionServer, percentile, run_plain, serving_mix,
                                       synthesize_request)
 
-    if int(os.environ.get("RANK", "0")) != 0:
-        return
-    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
-    torch.cuda.set_device(dev)
     _abi.load()
     mix = serving_mix(args.requests, seed=4, rate=20.0)
-    reqs = [synthesize_request(rid, m, t, size, seed=500 + rid, device=dev, iters=args.iters)
+    reqs = [synthesize_request(rid, m, t, size, seed=500 + rid, device=dev, iters=args.iters,
+                               target_ratio=args.target_ratio)
             for rid, m, t, size in mix]
     torch.cuda.synchronize(dev)
-    # warm-up: one small request of each modality builds plans and loads kernels
+    # warm-up: one small request of each modality and size class builds plans and loads kernels
     warm = [synthesize_request(1000 + i, m, 0.0, size, seed=900 + i, device=dev, iters=2)
-            for i, (_, m, _, size) in enumerate({m: (r, m, t, s) for r, m, t, s in mix}.values())]
+            for i, (_, m, _, size) in enumerate({(m, size.get("p", size.get("n"))): (r, m, t, size)
+                                                  for r, m, t, size in mix}.values())]
     ReconstructionServer(dev).run(warm, realtime=False)
     run_plain(warm, dev, realtime=False)
 
@@ -952,52 +1100,82 @@ def run_serving(args) -> None:
         reqs, realtime=True)
     t_served = time.perf_counter() - t0
     launches = _abi.query("ptx_launch_count") - launches0
+    native, t_native = run_native(reqs, warm, dev, args.max_active)
     clk = clocks.stop()
     t0 = time.perf_counter()
     plain = run_plain(reqs, dev, realtime=True)
     t_plain = time.perf_counter() - t0
-    native, t_native = run_native(reqs, warm, dev, args.max_active)
 
-    sweeps = sum(r.sweeps for r in served)
-    lat_s = [r.latency for r in served]
-    lat_p = [r.latency for r in plain]
-    rel_final = [abs(a.final_loss - b.final_loss) / abs(b.final_loss) for a, b in zip(served, plain)]
+    def summary(results, wall):
+        sweeps = sum(r.sweeps for r in results)
+        lat = [r.latency for r in results]
+        return {"wall_s": wall, "sweeps": sweeps, "sweeps_per_s": sweeps / wall, "p50_latency_s": percentile(lat, 50),
+                "p99_latency_s": percentile(lat, 99), "iterations_mean": sweeps / max(len(results), 1)}
+
+    def rel(a, b):
+        return max(abs(x.final_loss - y.final_loss) / abs(y.final_loss) for x, y in zip(a, b))
+
     by_mod = {}
     for r in reqs:
         by_mod[r.modality] = by_mod.get(r.modality, 0) + 1
+    sizes = sorted({(r.modality, tuple(r.aux0.shape)) for r in reqs})
+    s_rate = sum(r.sweeps for r in served) / t_served
+    n_rate = sum(r.sweeps for r in native) / t_native
+    p_rate = sum(r.sweeps for r in plain) / t_plain
+    return {
+        "requests": len(reqs), "arrival_rate_per_s": 20.0, "max_active": args.max_active,
+        "max_iterations_per_request": args.iters, "target_ratio": args.target_ratio, "mix": by_mod,
+        "sizes": [f"{m} {'x'.join(map(str, sh))}" for m, sh in sizes],
+        "mix_rule": "40/30/20/10% configs 0/2/3/1, sizes x U[0.75,1.25] (conventional probes {2,3,5}-smooth)",
+        "served": summary(served, t_served),
+        "native": summary(native, t_native),
+        "plain": summary(plain, t_plain),
+        "throughput_ratio_served_over_plain": s_rate / p_rate,
+        "throughput_ratio_native_over_plain": n_rate / p_rate,
+        "final_loss_rel_diff_max_served_vs_plain": rel(served, plain),
+        "final_loss_rel_diff_max_native_vs_plain": rel(native, plain),
+        "requests_stopped_at_target": {"served": sum(r.sweeps < args.iters for r in served),
+                                       "native": sum(r.sweeps < args.iters for r in native),
+                                       "plain": sum(r.sweeps < args.iters for r in plain)},
+        "gpu_launches_served": launches,
+        "clocks": clk,
+        "methods": {"served": "Python server: HBM-budget admission, resident state, one captured graph per "
+                              "reconstruction's iteration, concurrent replay on prioritised streams",
+                    "native": "the same service in libptychox (ptx_server_*): scheduler thread replaying, "
+                              "admission thread uploading / warming up / capturing / reading back; requests "
+                              "submitted at their arrival times",
+                    "plain": "one request at a time: unfused operators + F.mse_loss + torch.optim.Adam, the loss "
+                             "read every iteration when a target is set (the reference drivers' loop)"},
+    }
+
+
+def run_serving(args) -> None:
+    """The served mixed stream as its own bench line (``--workload serving-mix``)."""
+    import torch
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    rec = serving_record(args, dev)
+    served = rec["served"]
     line = {
         "metric": "served mixed stream: sweeps/s (p50/p99 latency alongside)",
-        "value": sweeps / t_served,
+        "value": served["sweeps_per_s"],
         "unit": "sweeps/s",
         "n_gpus": 1,
-        "steps": len(reqs),
-        "warmup": len(warm),
-        "ms_per_step": 1e3 * t_served / max(sweeps, 1),
+        "steps": rec["requests"],
+        "warmup": 0,
+        "ms_per_step": 1e3 / max(served["sweeps_per_s"], 1e-9),
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "c64 (FP32 FFT/constraint, FP64 loss sum)",
         "data": "synthetic (seeded problems, Poisson uint16 counts from the forward model)",
-        "config": {"workload": "serving-mix", "requests": len(reqs), "arrival_rate_per_s": 20.0,
-                   "max_active": args.max_active,
-                   "iterations_per_request": args.iters, "mix": by_mod,
-                   "mix_rule": "40/30/20/10% configs 0/2/3/1, sizes x U[0.75,1.25]"},
-        "served": {"wall_s": t_served, "sweeps_per_s": sweeps / t_served, "p50_latency_s": percentile(lat_s, 50),
-                   "p99_latency_s": percentile(lat_s, 99)},
-        "plain": {"wall_s": t_plain, "sweeps_per_s": sweeps / t_plain, "p50_latency_s": percentile(lat_p, 50),
-                  "p99_latency_s": percentile(lat_p, 99),
-                  "method": "one request at a time: unfused operators + F.mse_loss + torch.optim.Adam"},
-        "native": {"wall_s": t_native, "sweeps_per_s": sweeps / t_native,
-                   "p50_latency_s": percentile([r.latency for r in native], 50),
-                   "p99_latency_s": percentile([r.latency for r in native], 99),
-                   "final_loss_rel_diff_max_vs_served": max(abs(a.final_loss - b.final_loss) / abs(b.final_loss)
-                                                          for a, b in zip(native, served)),
-                   "method": "the same service in libptychox's scheduler thread (C ABI ptx_server_*), "
-                             "requests submitted at their arrival times and polled"},
-        "throughput_ratio_served_over_plain": t_plain / t_served,
-        "final_loss_rel_diff_max": max(rel_final),
-        "gpu_launches": launches,
-        "clocks": clk,
+        "config": {"workload": "serving-mix", "requests": rec["requests"], "mix": rec["mix"]},
+        "serving": rec,
+        "gpu_launches": rec["gpu_launches_served"],
+        "clocks": rec["clocks"],
     }
     print(json.dumps(line), flush=True)
 
@@ -1010,11 +1188,17 @@ def main() -> None:
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS) + ["serving-mix"])
     ap.add_argument("--requests", type=int, default=40)
     ap.add_argument("--iters", type=int, default=50)
+    ap.add_argument("--target-ratio", type=float, default=0.0,
+                    help="serving: stop a request once its loss is at most this fraction of its initial loss")
+    ap.add_argument("--no-serving", action="store_true",
+                    help="skip the served-stream record of the default line")
     ap.add_argument("--max-active", type=int, default=8)
     ap.add_argument("--units-per-cta", type=int, default=8,
                     help="serving: bound on the units a persistent-pass CTA takes (0: one wave)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own GPU paths (torch on CUDA, its CUDA extension)")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--units", type=int, default=0,
                     help="run the workload on its first N scan units only (small profiling cases)")
