@@ -17,8 +17,9 @@ the operator with ``use_cuda_kernels=False`` in complex64, ``F.mse_loss`` and
 ``.backward()``) on all host cores, one whole sweep per step; without that install it
 falls back to the oracle's numpy restatement (``kind: "port"``).
 
-With N > 1 (torchrun) each rank sweeps its own 900 positions over the shared object
-and the gradients are all-reduced over NCCL (data-parallel sweep, weak scaling).
+With N > 1 (torchrun) the ranks share one reconstruction: each sweeps its row band of the
+scan and the weighted loss and gradients are all-reduced over NCCL (strong scaling; the
+weak figure, every rank sweeping all positions, is reported beside it).
 """
 
 from __future__ import annotations
@@ -488,17 +489,30 @@ def run_ours(args) -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     _abi.load()
 
-    prob = wl.synth(seed=1000 + rank, dev=dev)
-    ws = wl.workspace(prob, dev)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    # Every rank synthesises the same problem.  Strong scaling (default with N > 1): the ranks
+    # share one reconstruction, each sweeping its row band of the scan (shard_positions) and
+    # all-reducing the weighted loss and gradients, so a step is one whole sweep.  Weak: every
+    # rank sweeps all units and the results are averaged (N sweeps per step).
+    from ptychox_b200.distributed import reduce_sweep, shard_positions
 
-    from ptychox_b200.distributed import reduce_sweep
+    strong = world > 1 and args.scaling == "strong"
+    prob = wl.synth(seed=1000, dev=dev)
+    full_prob = prob
+    local_units, total_units = wl.batch, wl.batch * (1 if strong else world)
+    if strong:
+        idx = shard_positions(prob["host"]["pos"], rank, world)
+        it = torch.from_numpy(idx).to(dev)
+        prob = dict(prob, pos=prob["pos"][it].contiguous(), meas=prob["meas"][it].contiguous(),
+                    host=dict(prob["host"], pos=np.ascontiguousarray(prob["host"]["pos"][idx])))
+        local_units = len(idx)
+    ws = wl.workspace(full_prob, dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
     def step():
         loss, g_obj, g_aux = wl.sweep(prob, ws)
         if world > 1:  # data-parallel sweep: global mean over all ranks' units
-            reduce_sweep(loss, [g_obj, g_aux], wl.batch, wl.batch * world)
-        return loss
+            reduce_sweep(loss, [g_obj, g_aux], local_units, total_units)
+        return loss, g_obj, g_aux
 
     def timed(k: int, fn) -> list[float]:
         pairs = []
@@ -541,7 +555,32 @@ def run_ours(args) -> None:
     clk = clocks.stop()
     total_ms = max_over_ranks(sum(step_ms))
     ms_per_step = total_ms / args.steps
-    value = world * args.steps / (total_ms / 1e3)
+    value = (1 if strong else world) * args.steps / (total_ms / 1e3)
+
+    multi = None
+    if world > 1:
+        # the sharded sweep equals the whole sweep on one GPU (checked on rank 0, no collective)
+        loss_r, go_r, ga_r = step()
+        torch.cuda.synchronize(dev)
+        multi = {"mode": "strong" if strong else "weak", "units_per_rank": local_units}
+        if strong and rank == 0:
+            loss_1, go_1, ga_1 = wl.sweep(full_prob, ws)
+            torch.cuda.synchronize(dev)
+            multi["parity_vs_one_gpu"] = {
+                "loss": abs(float(loss_r) - float(loss_1)) / abs(float(loss_1)),
+                "grad_obj": float((go_r - go_1).norm() / go_1.norm()),
+                "grad_aux": float((ga_r - ga_1).norm() / ga_1.norm())}
+        if strong:
+            # the weak figure beside it: every rank sweeps all units of the same problem
+
+            def weak_step():
+                loss, g_obj, g_aux = wl.sweep(full_prob, ws)
+                reduce_sweep(loss, [g_obj, g_aux], wl.batch, wl.batch * world)
+
+            dist.barrier()
+            weak_ms = max_over_ranks(sum(timed(args.steps, weak_step)))
+            multi["weak"] = {"value": world * args.steps / (weak_ms / 1e3), "unit": "sweeps/s",
+                             "ms_per_step": weak_ms / args.steps}
 
     # ---- roofline: the sweep's kernels timed with library events ------------------
     _abi.query("ptx_profile_reset")
@@ -551,7 +590,8 @@ def run_ours(args) -> None:
     per_kernel = _abi.profile_read()
     peak, peak_kind = hbm_peak()
     sweep_bytes = wl.bytes_per_sweep()
-    achieved = sweep_bytes / (ms_per_step / 1e3) / 1e9
+    # per GPU: the share of the sweep this rank moves in one step
+    achieved = sweep_bytes * (local_units / wl.batch) / (ms_per_step / 1e3) / 1e9
     kern_total = sum(v[0] for v in per_kernel.values()) or 1.0
     kernels = [{"name": k, "launches_per_step": n / args.steps, "ms_per_launch": ms / n, "share": ms / kern_total}
                for k, (ms, n) in sorted(per_kernel.items(), key=lambda kv: -kv[1][0])]
@@ -612,7 +652,7 @@ def run_ours(args) -> None:
             loss.backward()
             g_obj, g_aux, l_det = d_obj.grad, d_aux.grad, loss.detach()
             if world > 1:
-                reduce_sweep(l_det, [g_obj, g_aux], wl.batch, wl.batch * world)
+                reduce_sweep(l_det, [g_obj, g_aux], local_units, total_units)
             done = torch.cuda.Event()
             done.record(s_comp)
             freed[b] = done
@@ -641,7 +681,8 @@ def run_ours(args) -> None:
     e2e_ms = max_over_ranks(e2e_run(args.steps))
     h2d = (h_obj.numel() + h_aux.numel()) * 8 + h_pos.numel() * h_pos.element_size()
     d2h = (out_go[0].numel() + out_ga[0].numel()) * 8 + 8
-    e2e = {"value": world * args.steps / (e2e_ms / 1e3), "unit": "sweeps/s", "h2d_bytes_per_step": h2d,
+    e2e = {"value": (1 if strong else world) * args.steps / (e2e_ms / 1e3), "unit": "sweeps/s",
+           "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h,
            "note": "public loss API (autograd); each step uploads object, probe/pupil/mask and scan from pinned "
                    "host memory (the scan through the API's own pinned upload) and reads back the loss and "
@@ -669,7 +710,10 @@ def run_ours(args) -> None:
 
     if rank == 0:
         cfg = wl.config()
-        cfg["parallelism"] = f"dp{world} (per-rank positions, NCCL all-reduce of gradients)" if world > 1 else "single GPU"
+        cfg["parallelism"] = ((f"dp{world}: one reconstruction, row-band position shards, NCCL all-reduce of the "
+                               f"weighted loss and gradients" if strong else
+                               f"dp{world}: every rank sweeps all positions, NCCL all-reduce")
+                              if world > 1 else "single GPU")
         cfg["l2"] = "flushed between timed steps (256 MB write outside the step events)"
         line = {
             "metric": wl.metric(),
@@ -680,11 +724,12 @@ def run_ours(args) -> None:
             "warmup": args.warmup,
             "ms_per_step": ms_per_step,
             "higher_is_better": True,
-            "scaling": "weak",
+            "scaling": "strong" if strong else "weak",
             "vs_baseline": None,
             "dtype": "c64 (FP32 FFT/constraint, FP64 loss sum)",
             "data": "synthetic (seeded object and scan, Poisson uint16 counts from the forward model)",
             "config": cfg,
+            "multi_gpu": multi,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "cpu_baseline_port": cpu_port,
@@ -1183,6 +1228,8 @@ def run_serving(args) -> None:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--scaling", default="strong", choices=["strong", "weak"],
+                    help="N > 1: shard one reconstruction over the ranks (strong) or sweep all units on every rank")
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS) + ["serving-mix"])

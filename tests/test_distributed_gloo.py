@@ -26,6 +26,14 @@ def _problem(kind):
     from ptychox_b200 import synth
 
     rng = np.random.default_rng(21)
+    if kind == "base-config0":
+        # config 0 shape: 512^2 object, 128^2 probe, 11 x 11 raster step 32, U[-2, 2] jitter
+        obj = synth.random_object(512, 512, rng)
+        probe = synth.gaussian_probe(128, 128, rng)
+        pos = synth.raster_positions(11, 32, 8, 2, rng)
+        amp, _, _ = O.base_forward(obj, probe, pos)
+        meas, scale = synth.poisson_counts(amp**2, 1e4, rng)
+        return obj, probe, pos, meas, scale
     if kind == "base":
         obj = synth.random_object(96, 96, rng)
         probe = synth.gaussian_probe(32, 32, rng)
@@ -55,7 +63,7 @@ def _worker(rank, world, port, kind, out):
     try:
         obj, aux, pos, meas, scale = _problem(kind)
         idx = shard_positions(pos, rank, world)
-        sweep = O.base_sweep if kind == "base" else O.fpm_sweep
+        sweep = O.fpm_sweep if kind == "fpm" else O.base_sweep
         loss, g1, g2 = sweep(obj, aux, pos[idx], meas[idx], scale)
         t_loss = torch.tensor(loss, dtype=torch.float64)
         t1 = torch.from_numpy(np.ascontiguousarray(g1))
@@ -68,8 +76,10 @@ def _worker(rank, world, port, kind, out):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("kind", ["base", "fpm"])
+@pytest.mark.parametrize("kind", ["base", "fpm", "base-config0"])
 def test_two_rank_sweep_equals_single_process(kind):
+    """One reconstruction sharded over two ranks (row bands, uneven: 13 / 12, and 61 / 60 at the
+    config-0 shape) and reduced with reduce_sweep equals the single-process sweep."""
     from oracle import ptycho_oracle as O
 
     ctx = mp.get_context("spawn")
@@ -83,7 +93,7 @@ def test_two_rank_sweep_equals_single_process(kind):
         p.join(timeout=60)
         assert p.exitcode == 0
     obj, aux, pos, meas, scale = _problem(kind)
-    sweep = O.base_sweep if kind == "base" else O.fpm_sweep
+    sweep = O.fpm_sweep if kind == "fpm" else O.base_sweep
     rl, r1, r2 = sweep(obj, aux, pos, meas, scale)
     assert sum(sizes) == len(pos) and max(sizes) - min(sizes) <= 1
     assert abs(loss - rl) <= 1e-12 * abs(rl)
