@@ -230,8 +230,15 @@ struct ColPairCfg {
 
 // UNIT_NORM: `norm` is 1 (the epilogue drops the scaling); FULL: `width` is a multiple of
 // the tile, so every column pair exists and the per-column masks go.
+// Up to 256-point columns a CTA fits 128 registers per thread and 47 KB of shared memory, so
+// four CTAs share an SM (16 warps); longer columns keep two (512) or one (1024).
+template <int N>
+constexpr int col_pair_min_blocks() {
+  return ColPairCfg<N>::kThreads > 128 ? 1 : (N <= 256 ? 4 : 2);
+}
+
 template <int N, bool FIRST_INV, bool SHIFTED, bool UNIT_NORM = false, bool FULL = false>
-__global__ void __launch_bounds__(ColPairCfg<N>::kThreads, ColPairCfg<N>::kThreads <= 128 ? 2 : 1) cols_sweep_pair(
+__global__ void __launch_bounds__(ColPairCfg<N>::kThreads, col_pair_min_blocks<N>()) cols_sweep_pair(
     float2* __restrict__ scratch, int width, int frame0, const float2* __restrict__ tw,
     const uint16_t* __restrict__ measured, const float* __restrict__ lut, float norm, float grad_scale,
     double inv_numel, double* __restrict__ loss) {
