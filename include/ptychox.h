@@ -99,6 +99,12 @@ const char* ptx_profile_name(int kernel_id);
 /* 1 if `n` is a supported transform length (n = 2^a 3^b 5^c, 2 <= n <= 1024). */
 int ptx_fft_supported(int n);
 
+/* Which kernels serve line length `n` in the conventional passes: 1 for the power-of-two
+ * register FFT (16 .. 1024), 2 for the mixed-radix register FFT (the 2^a 3^b 5^c lengths
+ * 6 .. 1000 that are not powers of two), 3 for the runtime-plan shared-memory FFT (the
+ * remaining supported lengths 2 .. 8), 0 for an unsupported length.  Host-only query. */
+int ptx_fft_engine(int n);
+
 /* Build the twiddle table for length n on the current device now (it is otherwise
  * built on first use, which must not happen inside a CUDA graph capture). */
 int ptx_fft_prepare(int n);

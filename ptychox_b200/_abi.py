@@ -50,6 +50,7 @@ SIGNATURES: dict[str, tuple] = {
     "ptx_profile_read": (_i, [_i, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
     "ptx_profile_name": (C.c_char_p, [_i]),
     "ptx_fft_supported": (_i, [_i]),
+    "ptx_fft_engine": (_i, [_i]),
     "ptx_fft_prepare": (_i, [_i]),
     "ptx_base_workspace_bytes": (_sz, [_i, _i, _i]),
     "ptx_base_forward": (_i, [_p, _i, _i, _p, _i, _i, _p, _i, _p, _p, _p, _sz, _p]),

@@ -796,7 +796,9 @@ int check_common(const void* sample, int H, int W, const void* probe, int ph, in
                      ws_bytes, kHeaderBytes + g->frame_bytes);
   }
   size_t fit = (ws_bytes - kHeaderBytes) / g->frame_bytes;
-  g->chunk = static_cast<int>(std::min<size_t>(fit, (size_t)std::max(batch, 1)));
+  // frames of one chunk: what the workspace holds, at most the batch, and at most 65535
+  // (the column passes put the frame in gridDim.y)
+  g->chunk = static_cast<int>(std::min<size_t>({fit, (size_t)std::max(batch, 1), (size_t)65535}));
   g->err = reinterpret_cast<unsigned*>(ws);
   g->lut = reinterpret_cast<float*>(static_cast<char*>(ws) + 256);
   g->scratch = reinterpret_cast<float2*>(static_cast<char*>(ws) + kHeaderBytes);
@@ -807,6 +809,8 @@ int check_common(const void* sample, int H, int W, const void* probe, int ph, in
       using L = RegLaunch<N>;
       if (!st) st = ensure_smem((const void*)base_rows_forward_reg<N>, FwdCfg<N>::smem(L::lines(128, ph)));
       if (!st) st = ensure_smem((const void*)base_rows_adjoint_reg<N>, L::adj_smem(L::lines(128, ph)));
+    } else if (const MixOps* mo = mix_ops(pw)) {
+      if (!st) st = mo->prepare();
     } else {
       if (!st) st = ensure_smem((const void*)base_rows_forward_rt<0>, g->rs.smem);
       if (!st) st = ensure_smem((const void*)base_rows_adjoint_rt<0>, g->rs.smem);
@@ -820,6 +824,8 @@ int check_common(const void* sample, int H, int W, const void* probe, int ph, in
       if (!st) st = ensure_smem((const void*)cols_sweep_pair<N, false, true, true, true>, ColPairCfg<N>::kSmemBytes);
       if (!st) st = ensure_smem((const void*)base_cols_reg<kColForward, N>, sm);
       if (!st) st = ensure_smem((const void*)base_cols_reg<kColBackward, N>, sm);
+    } else if (const MixOps* mo = mix_ops(ph)) {
+      if (!st) st = mo->prepare();
     } else {
       if (!st) st = ensure_smem((const void*)base_cols_rt<kColSweep, 0>, g->cs.smem);
       if (!st) st = ensure_smem((const void*)base_cols_rt<kColForward, 0>, g->cs.smem);
@@ -849,6 +855,10 @@ void launch_rows_forward(const BaseGeom& g, const float2* sample, const float2* 
       const int grid = persistent_grid((const void*)base_rows_forward_reg<N>, threads, smem, (long long)rowgroups * nframes);
       base_rows_forward_reg<N><<<grid, threads, smem, s>>>(sample, g.H, g.W, probe, g.ph, pos, nframes, rowgroups,
                                                            g.scratch, g.row.tw, lines, g.err);
+    } else if (const MixOps* mo = mix_ops(g.pw)) {
+      MixRowsArgs a{sample, g.H, g.W, probe, g.ph, g.pw, pos, nframes, g.scratch, g.row.mix_twt, g.row.mix_twi,
+                    g.err, nullptr, nullptr};
+      mo->rows_forward(a, s);
     } else {
       const int rowgroups = (g.ph + g.rs.lines - 1) / g.rs.lines;
       dim3 grid(rowgroups, nframes);
@@ -873,6 +883,10 @@ void launch_rows_adjoint(const BaseGeom& g, const float2* sample, const float2* 
       const int grid = persistent_grid((const void*)base_rows_adjoint_reg<N>, threads, smem, units);
       base_rows_adjoint_reg<N><<<grid, threads, smem, s>>>(g.scratch, sample, g.H, g.W, probe, g.ph, pos, nframes,
                                                            rowgroups, grad_sample, grad_probe, g.row.tw, lines);
+    } else if (const MixOps* mo = mix_ops(g.pw)) {
+      MixRowsArgs a{sample, g.H, g.W, probe, g.ph, g.pw, pos, nframes, g.scratch, g.row.mix_twt, g.row.mix_twi,
+                    g.err, grad_sample, grad_probe};
+      mo->rows_adjoint(a, s);
     } else {
       const int rowgroups = (g.ph + g.rs.lines - 1) / g.rs.lines;
       const int fpc = frames_per_cta_for(rowgroups, nframes, sm_count() * 8);
@@ -910,6 +924,10 @@ void launch_cols(const BaseGeom& g, int frame0, int nframes, const uint16_t* mea
       base_cols_reg<MODE, N><<<grid, L::col_threads(), L::col_smem(), s>>>(
           g.scratch, g.pw, frame0, g.col.tw, measured, g.lut, grad_scale, inv_numel, loss, far_field, amplitude,
           grad_output);
+    } else if (const MixOps* mo = mix_ops(g.ph)) {
+      MixColsArgs a{g.scratch, g.ph, g.pw, frame0, nframes, g.col.mix_twt, g.col.mix_twi, measured, g.lut,
+                    grad_scale, inv_numel, loss, far_field, amplitude, grad_output};
+      mo->cols(MODE == kColSweep ? kMixColSweep : MODE == kColForward ? kMixColForward : kMixColBackward, a, s);
     } else {
       dim3 grid(num_tiles(g.pw) * (kTile / g.cs.cols), nframes);
       base_cols_rt<MODE, 0><<<grid, g.cs.threads, g.cs.smem, s>>>(g.scratch, g.ph, g.pw, frame0, g.col,
@@ -938,6 +956,8 @@ int base_cols_pass(bool forward, float2* scratch, int ph, int pw, int frame0, in
       const int sm = RegLaunch<N>::col_smem();
       st = ensure_smem(forward ? (const void*)base_cols_reg<kColForward, N> : (const void*)base_cols_reg<kColBackward, N>,
                        sm);
+    } else if (const MixOps* mo = mix_ops(ph)) {
+      st = mo->prepare();
     } else {
       st = ensure_smem(forward ? (const void*)base_cols_rt<kColForward, 0> : (const void*)base_cols_rt<kColBackward, 0>,
                        g.cs.smem);

@@ -22,18 +22,19 @@
 #include <vector>
 
 #include "ptx_internal.h"
+#include "ptx_mixfft.cuh"
 
 namespace ptx {
 
 namespace {
 
-constexpr int kPoolEntries = 1 << 16;  // 512 KB of float2 per device
+constexpr int kPoolEntries = 1 << 17;  // 1 MB of float2 per device
 __device__ float2 g_twiddle_pool[kPoolEntries];
 
 thread_local std::string g_last_error;
 
 std::mutex g_plan_mutex;
-std::map<int, int> g_table_offset;                       // n -> offset in the pool
+std::map<int, int> g_table_offset;                       // n -> offset of n's tables in the pool
 int g_pool_used = 0;
 std::map<std::pair<int, int>, LinePlan> g_plans;         // (device, n) -> plan
 
@@ -112,25 +113,40 @@ int get_line_plan(int n, LinePlan* out) {
   p.nstages = make_radices(n, radix);
   p.radices = 0;
   for (int s = 0; s < p.nstages; ++s) p.radices |= static_cast<unsigned long long>(radix[s]) << (5 * s);
+  // the natural table (n entries), then for mixed-radix lengths the two layouts of the
+  // inter-step twiddles (n entries each)
+  const int mix_b = (n & (n - 1)) ? mix::split_b(n) : 0;
+  const int entries = mix_b ? 3 * n : n;
   int offset;
   auto ot = g_table_offset.find(n);
   if (ot == g_table_offset.end()) {
-    if (g_pool_used + n > kPoolEntries) {
+    const int span = (entries + 31) / 32 * 32;
+    if (g_pool_used + span > kPoolEntries) {
       return set_error(PTX_ERR_UNSUPPORTED_SIZE, "twiddle pool exhausted (call ptx_clear_cache)");
     }
     offset = g_pool_used;
-    g_pool_used += (n + 31) / 32 * 32;
+    g_pool_used += span;
     g_table_offset[n] = offset;
   } else {
     offset = ot->second;
   }
-  std::vector<float2> table(n);
+  std::vector<float2> table(entries);
   const double two_pi = 6.283185307179586476925286766559;
   for (int m = 0; m < n; ++m) {
     const double ang = two_pi * static_cast<double>(m) / static_cast<double>(n);
     table[m] = make_float2(static_cast<float>(std::cos(ang)), static_cast<float>(-std::sin(ang)));
   }
-  if (int st = cuda_status(cudaMemcpyToSymbol(g_twiddle_pool, table.data(), sizeof(float2) * n,
+  if (mix_b) {
+    const int a = n / mix_b;
+    for (int t = 0; t < mix_b; ++t) {
+      for (int u = 0; u < a; ++u) {
+        const float2 w = table[(t * u) % n];
+        table[n + u * mix_b + t] = w;
+        table[2 * n + t * a + u] = w;
+      }
+    }
+  }
+  if (int st = cuda_status(cudaMemcpyToSymbol(g_twiddle_pool, table.data(), sizeof(float2) * entries,
                                               sizeof(float2) * offset, cudaMemcpyHostToDevice),
                            "twiddle upload")) {
     return st;
@@ -140,6 +156,8 @@ int get_line_plan(int n, LinePlan* out) {
     return st;
   }
   p.tw = reinterpret_cast<const float2*>(base) + offset;
+  p.mix_twt = mix_b ? p.tw + n : nullptr;
+  p.mix_twi = mix_b ? p.tw + 2 * n : nullptr;
   g_plans[key] = p;
   *out = p;
   return PTX_OK;
@@ -489,6 +507,12 @@ const char* ptx_profile_name(int kernel_id) {
 }
 
 int ptx_fft_supported(int n) { return ptx::size_supported(n) ? 1 : 0; }
+
+int ptx_fft_engine(int n) {
+  if (!ptx::size_supported(n)) return 0;
+  if (n >= 16 && (n & (n - 1)) == 0) return 1;
+  return ptx::mix_ops(n) ? 2 : 3;
+}
 
 int ptx_fft_prepare(int n) {
   ptx::LinePlan p;

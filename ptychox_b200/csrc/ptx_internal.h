@@ -129,4 +129,44 @@ void dispatch_len(int n, F&& f) {
   }
 }
 
+// ---- conventional passes on the mixed-radix register FFT (ptx_mix.cuh) ---------------
+// Compiled for a list of {2,3,5}-smooth lengths that are not powers of two; mix_ops(n)
+// is null for every other length (those run the runtime-plan kernels).
+struct MixRowsArgs {
+  const float2* sample;  // object, H x W
+  int H, W;
+  const float2* probe;   // ph x pw
+  int ph, pw;
+  const int64_t* pos;    // (x, y) of each frame's window
+  int nframes;
+  float2* scratch;       // tiled frames [frame][tile][row][16]
+  const float2* twt;     // row-length twiddles (LinePlan::mix_twt / mix_twi)
+  const float2* twi;
+  unsigned* err;         // window error word (forward pass)
+  float2* grad_sample;   // adjoint pass outputs (float2 atomics)
+  float2* grad_probe;
+};
+struct MixColsArgs {
+  float2* scratch;
+  int ph, pw, frame0, nframes;
+  const float2* twt;     // column-length twiddles
+  const float2* twi;
+  const uint16_t* measured;  // sweep: fftshifted counts
+  const float* lut;          // sweep: count -> observed amplitude
+  float grad_scale;
+  double inv_numel;
+  double* loss;
+  float2* far_field;         // forward: optional output; backward: input
+  float* amplitude;          // forward output
+  const float* grad_output;  // backward input
+};
+enum MixColMode { kMixColSweep = 0, kMixColForward = 1, kMixColBackward = 2 };
+struct MixOps {
+  int (*prepare)();  // raise the dynamic shared memory limits of the kernels
+  void (*rows_forward)(const MixRowsArgs&, cudaStream_t);
+  void (*rows_adjoint)(const MixRowsArgs&, cudaStream_t);
+  void (*cols)(int mode, const MixColsArgs&, cudaStream_t);
+};
+const MixOps* mix_ops(int n);
+
 }  // namespace ptx

@@ -46,6 +46,14 @@ def test_pure_host_entry_points(lib):
         assert lib.ptx_fft_supported(n) == 1, n
     for n in (0, 1, 7, 14, 2048, 1025):
         assert lib.ptx_fft_supported(n) == 0, n
+    # which FFT engine serves each length: every smooth length 6..1000 that is not a power of
+    # two has compiled mixed-radix kernels; only 2, 3, 4, 5 and 8 are left to the runtime plan
+    smooth = [n for n in range(2, 1025) if lib.ptx_fft_supported(n)]
+    engines = {n: lib.ptx_fft_engine(n) for n in smooth}
+    assert [n for n, e in engines.items() if e == 1] == [16, 32, 64, 128, 256, 512, 1024]
+    assert [n for n, e in engines.items() if e == 3] == [2, 3, 4, 5, 8]
+    assert all(e == 2 for n, e in engines.items() if n >= 6 and n & (n - 1))
+    assert lib.ptx_fft_engine(7) == 0 and lib.ptx_fft_engine(2048) == 0
     hdr = 256 + 65536 * 4  # error word + count-decode table
     ws = lib.ptx_base_workspace_bytes(512, 512, 900)
     frame = 512 * 512 * 8
