@@ -61,10 +61,14 @@ struct RowCfg {
   static constexpr int LINES = 256 / B > 0 ? 256 / B : 1;
   static constexpr int THREADS = LINES * B;
   static constexpr int BUF = A * P + (((B - A * P) % 16) + 16) % 16;
-  // forward: exchange buffers; adjoint: exchange buffers and the inverse twiddle table
+  // adjoint landing lines: one scratch row per line, 16-byte aligned
+  static constexpr int LAND = (N + 1) / 2 * 2;
+  // forward: exchange buffers; adjoint: exchange buffers, the inverse twiddle table and the
+  // landing lines
   static int smem_forward(int lines) { return lines * BUF * (int)sizeof(float2); }
-  static int smem_adjoint(int lines) { return (lines * BUF + N) * (int)sizeof(float2); }
-  static constexpr int SMEM_MAX = (LINES * BUF + N) * (int)sizeof(float2);
+  __host__ __device__ static constexpr int land_offset(int lines) { return (lines * BUF + N + 1) / 2 * 2; }
+  static int smem_adjoint(int lines) { return (land_offset(lines) + lines * LAND) * (int)sizeof(float2); }
+  static constexpr int SMEM_MAX = (land_offset(LINES) + LINES * LAND) * (int)sizeof(float2);
 };
 
 // Column pass: C columns of one frame tile per CTA, thread (t, c) at t * C + c; the C lines
@@ -124,8 +128,10 @@ __global__ void __launch_bounds__(RowCfg<N>::THREADS) mix_rows_forward(MixRowsAr
 }
 
 // ---- rows adjoint: grid (frame chunks, row groups), `fpc` frames per CTA -------------------
-// The grad_P partials stay in registers across the CTA's frames; the twiddles are read from
-// a shared-memory copy and the probe through ld_nc_here, so neither is held in registers.
+// Each line's scratch row of the next frame lands in shared memory by 16-byte cp.async (L2
+// evict-first: read once) while the current frame scatters.  The grad_P partials stay in
+// registers across the CTA's frames; the twiddles are read from a shared-memory copy and the
+// probe through ld_nc_here, so neither is held in registers.
 template <int N>
 __global__ void __launch_bounds__(RowCfg<N>::THREADS, 2) mix_rows_adjoint(MixRowsArgs a, int lines, int fpc) {
   using Cfg = RowCfg<N>;
@@ -140,29 +146,43 @@ __global__ void __launch_bounds__(RowCfg<N>::THREADS, 2) mix_rows_adjoint(MixRow
   const int f1 = min(a.nframes, f0 + fpc);
   float2* buf = sm + l * Cfg::BUF;
   float2* twi_s = sm + lines * Cfg::BUF;
+  float2* land = sm + Cfg::land_offset(lines) + l * Cfg::LAND;
+  const size_t frame_stride = (size_t)num_tiles(N) * a.ph * kTile;
+  const uint64_t pol_first = policy_evict_first();
+  // scratch row r of frame f -> land[0, N): pairs of elements (a tile row holds 16)
+  auto prefetch = [&](int f) {
+    const float2* src = a.scratch + (size_t)f * frame_stride + (size_t)r * kTile;
+    const int tq = t + opaque_zero();
+#pragma unroll
+    for (int i = 0; i < (N / 2 + B - 1) / B; ++i) {
+      const int kc = 2 * (tq + B * i);
+      if (kc + 1 < N) cp_async16_hint(land + kc, src + (kc / kTile) * a.ph * kTile + (kc % kTile), pol_first);
+    }
+    if ((N & 1) && t == 0) cp_async8_hint(land + N - 1, src + ((N - 1) / kTile) * a.ph * kTile + ((N - 1) % kTile), pol_first);
+    cp_async_commit();
+  };
   for (int i = tid; i < N; i += blockDim.x) twi_s[i] = __ldg(a.twi + i);
-  __syncthreads();
+  if (row_ok && f0 < f1) prefetch(f0);
   float2 acc[A];
 #pragma unroll
   for (int j = 0; j < A; ++j) acc[j] = make_float2(0.f, 0.f);
+  cp_async_wait_all();
+  __syncthreads();
   for (int f = f0; f < f1; ++f) {
     const long long x0 = a.pos[2 * f], y0 = a.pos[2 * f + 1];
     const bool ok = window_in(x0, y0, a.ph, N, a.H, a.W);
-    const int tz = t + opaque_zero();  // per-trip offsets (see opaque_zero)
     if (t < A && row_ok) {
-      const float2* base = a.scratch + (size_t)f * num_tiles(N) * a.ph * kTile + (size_t)r * kTile;
       float2 z[B];
 #pragma unroll
-      for (int k = 0; k < B; ++k) {
-        const int kc = tz + A * k;
-        z[k] = base[(kc / kTile) * a.ph * kTile + (kc % kTile)];
-      }
+      for (int k = 0; k < B; ++k) z[k] = land[t + A * k];
       mix::inv_step1<N, Cfg::P, 1>(z, buf, t, twi_s);
     }
-    __syncthreads();
+    __syncthreads();  // the exchange rows are complete and the landing line is free
+    if (row_ok && f + 1 < f1) prefetch(f + 1);
     if (row_ok && ok) {
       float2 y[A];
       mix::inv_step2<N, Cfg::P, 1>(y, buf, t);
+      const int tz = t + opaque_zero();  // per-trip offsets (see opaque_zero)
       const float2* orow = a.sample + (y0 + r) * a.W + x0;
       float2* grow = a.grad_sample + (y0 + r) * a.W + x0;
       const float2* prow = a.probe + (size_t)r * N;
@@ -173,7 +193,8 @@ __global__ void __launch_bounds__(RowCfg<N>::THREADS, 2) mix_rows_adjoint(MixRow
         acc[j] = cadd(acc[j], cmulc(y[j], __ldg(orow + c)));
       }
     }
-    __syncthreads();
+    cp_async_wait_all();
+    __syncthreads();  // the exchange rows are read and the next landing line is complete
   }
   if (row_ok && f0 < f1) {
 #pragma unroll
@@ -239,6 +260,7 @@ __global__ void __launch_bounds__(ColCfg<N>::THREADS) mix_cols(MixColsArgs a) {
     if (t < A) mix::fwd_step2<N, Cfg::RS, C>(z, buf, t);
   }
 
+  __shared__ double red_s[Cfg::THREADS / 32 + 1];
   if (MODE == kMixColSweep) {
     float part = 0.f;
     if (t < A) {
@@ -257,7 +279,15 @@ __global__ void __launch_bounds__(ColCfg<N>::THREADS) mix_cols(MixColsArgs a) {
         z[k] = out;
       }
     }
-    block_add_double(static_cast<double>(part), a.inv_numel, a.loss);
+    if constexpr (Cfg::THREADS % 32 == 0) {
+      // warp partials now; their sum after the barrier that the inverse transform needs anyway
+      double w = static_cast<double>(part);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+      if ((tid & 31) == 0) red_s[tid >> 5] = w;
+    } else {
+      block_add_double(static_cast<double>(part), a.inv_numel, a.loss);
+    }
   } else if (MODE == kMixColForward) {
     if (t < A && col_ok) {
 #pragma unroll
@@ -289,6 +319,14 @@ __global__ void __launch_bounds__(ColCfg<N>::THREADS) mix_cols(MixColsArgs a) {
   // thread u < A wrote and reads only row u of the exchange buffer since the last barrier
   if (t < A) mix::inv_step1<N, Cfg::RS, C>(z, buf, t, a.twi);
   __syncthreads();
+  if constexpr (MODE == kMixColSweep && Cfg::THREADS % 32 == 0) {
+    if (tid == 0) {
+      double w = 0.0;
+#pragma unroll
+      for (int i = 0; i < Cfg::THREADS / 32; ++i) w += red_s[i];
+      atomicAdd(a.loss, w * a.inv_numel);
+    }
+  }
   float2 y[A];
   mix::inv_step2<N, Cfg::RS, C>(y, buf, t);
   if (col_ok) {

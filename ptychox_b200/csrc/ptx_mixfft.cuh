@@ -86,8 +86,39 @@ struct Root {
 
 // ---- complex helpers (host and device) ------------------------------------------------
 
-PTX_MIX_HD float2 add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-PTX_MIX_HD float2 sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// Complex add / subtract and real-scalar FMA as single packed FP32x2 instructions on sm_100
+// (a - b as fma(b, -1, a), which rounds once exactly like the subtraction); plain FP32 on
+// the host.
+PTX_MIX_HD float2 add(float2 a, float2 b) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+  return __fadd2_rn(a, b);
+#else
+  return make_float2(a.x + b.x, a.y + b.y);
+#endif
+}
+PTX_MIX_HD float2 sub(float2 a, float2 b) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+  return __ffma2_rn(b, make_float2(-1.f, -1.f), a);
+#else
+  return make_float2(a.x - b.x, a.y - b.y);
+#endif
+}
+// s * b + a for real s
+PTX_MIX_HD float2 axpy(float s, float2 b, float2 a) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+  return __ffma2_rn(make_float2(s, s), b, a);
+#else
+  return make_float2(fmaf(s, b.x, a.x), fmaf(s, b.y, a.y));
+#endif
+}
+// s * b for real s
+PTX_MIX_HD float2 scale(float s, float2 b) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+  return __fmul2_rn(make_float2(s, s), b);
+#else
+  return make_float2(s * b.x, s * b.y);
+#endif
+}
 PTX_MIX_HD float2 mul(float2 a, float2 b) {
   return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
 }
@@ -152,10 +183,10 @@ struct Dft<3, INV> {
     constexpr float r3 = 0.86602540378443865f;  // sin(2 pi / 3)
     const float2 t = add(v[1], v[2]);
     const float2 d = rot<INV>(sub(v[1], v[2]));
-    const float2 m = make_float2(fmaf(-0.5f, t.x, v[0].x), fmaf(-0.5f, t.y, v[0].y));
+    const float2 m = axpy(-0.5f, t, v[0]);
     v[0] = add(v[0], t);
-    v[1] = make_float2(fmaf(r3, d.x, m.x), fmaf(r3, d.y, m.y));
-    v[2] = make_float2(fmaf(-r3, d.x, m.x), fmaf(-r3, d.y, m.y));
+    v[1] = axpy(r3, d, m);
+    v[2] = axpy(-r3, d, m);
   }
 };
 
@@ -184,10 +215,10 @@ struct Dft<5, INV> {
     const float2 da = sub(v[1], v[4]);
     const float2 sb = add(v[2], v[3]);
     const float2 db = sub(v[2], v[3]);
-    const float2 a1 = make_float2(fmaf(c2, sb.x, fmaf(c1, sa.x, v[0].x)), fmaf(c2, sb.y, fmaf(c1, sa.y, v[0].y)));
-    const float2 a2 = make_float2(fmaf(c1, sb.x, fmaf(c2, sa.x, v[0].x)), fmaf(c1, sb.y, fmaf(c2, sa.y, v[0].y)));
-    const float2 b1 = rot<INV>(make_float2(fmaf(s2, db.x, s1 * da.x), fmaf(s2, db.y, s1 * da.y)));
-    const float2 b2 = rot<INV>(make_float2(fmaf(-s1, db.x, s2 * da.x), fmaf(-s1, db.y, s2 * da.y)));
+    const float2 a1 = axpy(c2, sb, axpy(c1, sa, v[0]));
+    const float2 a2 = axpy(c1, sb, axpy(c2, sa, v[0]));
+    const float2 b1 = rot<INV>(axpy(s2, db, scale(s1, da)));
+    const float2 b2 = rot<INV>(axpy(-s1, db, scale(s2, da)));
     v[0] = add(v[0], add(sa, sb));
     v[1] = add(a1, b1);
     v[4] = sub(a1, b1);
