@@ -788,6 +788,9 @@ int check_common(const void* sample, int H, int W, const void* probe, int ph, in
   g->H = H; g->W = W; g->ph = ph; g->pw = pw; g->batch = batch;
   if (int st = get_line_plan(pw, &g->row)) return st;
   if (int st = get_line_plan(ph, &g->col)) return st;
+  if ((mix_ops(pw) && !g->row.mix_twt) || (mix_ops(ph) && !g->col.mix_twt)) {
+    return set_error(PTX_ERR_UNSUPPORTED_SIZE, "no mixed-radix twiddle tables for %d x %d", ph, pw);
+  }
   g->rs = row_shape(g->row, ph);
   g->cs = col_shape(g->col);
   g->frame_bytes = (size_t)num_tiles(pw) * kTile * ph * sizeof(float2);
@@ -948,6 +951,9 @@ int base_cols_pass(bool forward, float2* scratch, int ph, int pw, int frame0, in
   g.pw = pw;
   g.scratch = scratch;
   if (int st = get_line_plan(ph, &g.col)) return st;
+  if (mix_ops(ph) && !g.col.mix_twt) {
+    return set_error(PTX_ERR_UNSUPPORTED_SIZE, "no mixed-radix twiddle tables for length %d", ph);
+  }
   g.cs = col_shape(g.col);
   int st = PTX_OK;
   dispatch_len(ph, [&](auto NT) {
