@@ -297,42 +297,55 @@ struct Shape {
 // Twiddle tables, both of N entries: twt[u * B + t] = twi[t * A + u] = exp(-2 pi i t u / N)
 // (one per layout, so each step reads consecutive entries from consecutive threads).
 
-// Forward step 1, thread t < B: DFT-A of x[t + B j] (in y, j < A), twiddle, store row u.
-template <int N, int RS, int CS>
+// The steps below take the sign of the transform as PLUS: exp(-2 pi i ...) for PLUS = false
+// (the forward DFT), exp(+2 pi i ...) for PLUS = true (the unnormalised inverse).  "fwd" steps
+// map the space layout to the frequency layout, "inv" steps map back; both exist in both
+// signs (a forward transform after an inverse one, as the FPM column pass needs, is an "inv"
+// pair with PLUS = false).
+
+// Space -> frequency, step 1, thread t < B: DFT-A of x[t + B j] (in y, j < A), twiddle,
+// store row u.
+template <int N, int RS, int CS, bool PLUS = false>
 PTX_MIX_HD void fwd_step1(float2 (&y)[Shape<N>::A], float2* buf, int t, const float2* twt) {
   using S = Shape<N>;
-  Dft<S::A, false>::run(y);
+  Dft<S::A, PLUS>::run(y);
   buf[t * CS] = y[0];
 #pragma unroll
-  for (int u = 1; u < S::A; ++u) buf[u * RS + t * CS] = mul(y[u], twt[u * S::B + t]);
+  for (int u = 1; u < S::A; ++u) {
+    const float2 w = twt[u * S::B + t];
+    buf[u * RS + t * CS] = PLUS ? mulc(y[u], w) : mul(y[u], w);
+  }
 }
 
-// Forward step 2, thread u < A: DFT-B over row u -> z[k] = X[u + A k].
-template <int N, int RS, int CS>
+// Space -> frequency, step 2, thread u < A: DFT-B over row u -> z[k] = X[u + A k].
+template <int N, int RS, int CS, bool PLUS = false>
 PTX_MIX_HD void fwd_step2(float2 (&z)[Shape<N>::B], const float2* buf, int u) {
   using S = Shape<N>;
 #pragma unroll
   for (int k = 0; k < S::B; ++k) z[k] = buf[u * RS + k * CS];
-  Dft<S::B, false>::run(z);
+  Dft<S::B, PLUS>::run(z);
 }
 
-// Inverse step 1, thread u < A: inverse DFT-B of X[u + A k] (in z), conjugate twiddle, store row u.
-template <int N, int RS, int CS>
+// Frequency -> space, step 1, thread u < A: DFT-B of X[u + A k] (in z), twiddle, store row u.
+template <int N, int RS, int CS, bool PLUS = true>
 PTX_MIX_HD void inv_step1(float2 (&z)[Shape<N>::B], float2* buf, int u, const float2* twi) {
   using S = Shape<N>;
-  Dft<S::B, true>::run(z);
+  Dft<S::B, PLUS>::run(z);
   buf[u * RS] = z[0];
 #pragma unroll
-  for (int t = 1; t < S::B; ++t) buf[u * RS + t * CS] = mulc(z[t], twi[t * S::A + u]);
+  for (int t = 1; t < S::B; ++t) {
+    const float2 w = twi[t * S::A + u];
+    buf[u * RS + t * CS] = PLUS ? mulc(z[t], w) : mul(z[t], w);
+  }
 }
 
-// Inverse step 2, thread t < B: inverse DFT-A over column t -> y[j] = x[t + B j] (times N).
-template <int N, int RS, int CS>
+// Frequency -> space, step 2, thread t < B: DFT-A over column t -> y[j] = x[t + B j].
+template <int N, int RS, int CS, bool PLUS = true>
 PTX_MIX_HD void inv_step2(float2 (&y)[Shape<N>::A], const float2* buf, int t) {
   using S = Shape<N>;
 #pragma unroll
   for (int u = 0; u < S::A; ++u) y[u] = buf[u * RS + t * CS];
-  Dft<S::A, true>::run(y);
+  Dft<S::A, PLUS>::run(y);
 }
 
 }  // namespace mix

@@ -1,8 +1,9 @@
 // Host run of the mixed-radix two-step FFT steps (ptx_mixfft.cuh) against an FP64 DFT.
 //
 // For each length N the B "threads" of step 1 and the A "threads" of step 2 run one after
-// the other, in both buffer layouts (lines one after another; C = 8 lines interleaved).
-// Prints one line per length: N, forward error, inverse error (relative RMS), and the
+// the other, in both buffer layouts (lines one after another; C = 8 lines interleaved) and
+// both signs of each direction.  Prints one line per length: N, A, B, the space -> frequency
+// and frequency -> space errors (relative RMS, worst of the layouts and signs), and the
 // in-register DFT error of the factors A and B.
 #include <cmath>
 #include <complex>
@@ -106,6 +107,30 @@ static void run_layout(std::mt19937& rng, int c, double* efwd, double* einv) {
   }
   for (int i = 0; i < N; ++i) want[i] = x[i] * static_cast<double>(N);
   *einv = rel(back, want);
+  // the opposite signs: space -> frequency with exp(+i), frequency -> space with exp(-i)
+  for (int t = 0; t < S::B; ++t) {
+    float2 y[S::A];
+    for (int j = 0; j < S::A; ++j) y[j] = xf[t + S::B * j];
+    fwd_step1<N, RS, CS, true>(y, line, t, twt.data());
+  }
+  for (int u = 0; u < S::A; ++u) {
+    float2 z[S::B];
+    fwd_step2<N, RS, CS, true>(z, line, u);
+    for (int k = 0; k < S::B; ++k) got[u + S::A * k] = cd(z[k].x, z[k].y);
+  }
+  *efwd = std::max(*efwd, rel(got, dft(x, +1)));
+  for (int u = 0; u < S::A; ++u) {
+    float2 z[S::B];
+    for (int k = 0; k < S::B; ++k) z[k] = xf[u + S::A * k];
+    inv_step1<N, RS, CS, false>(z, line, u, twi.data());
+  }
+  const std::vector<cd> fw = dft(x, -1);
+  for (int t = 0; t < S::B; ++t) {
+    float2 y[S::A];
+    inv_step2<N, RS, CS, false>(y, line, t);
+    for (int j = 0; j < S::A; ++j) back[t + S::B * j] = cd(y[j].x, y[j].y);
+  }
+  *einv = std::max(*einv, rel(back, fw));
 }
 
 template <int N>
@@ -126,9 +151,9 @@ static void run_all(std::mt19937& rng) {
 
 int main() {
   std::mt19937 rng(7);
-  run_all<6, 9, 10, 12, 15, 18, 20, 24, 25, 27, 30, 36, 40, 45, 48, 50, 54, 60, 72, 75, 80, 81, 90, 96, 100, 108,
-          120, 125, 135, 144, 150, 160, 162, 180, 192, 200, 216, 225, 240, 243, 250, 270, 288, 300, 320, 324, 360,
-          375, 384, 400, 405, 432, 450, 480, 486, 500, 540, 576, 600, 625, 640, 648, 675, 720, 729, 750, 768, 800,
-          810, 864, 900, 960, 972, 1000>(rng);
+  run_all<4, 5, 6, 8, 9, 10, 12, 15, 16, 18, 20, 24, 25, 27, 30, 32, 36, 40, 45, 48, 50, 54, 60, 64, 72, 75, 80, 81, 90, 96,
+          100, 108, 120, 125, 128, 135, 144, 150, 160, 162, 180, 192, 200, 216, 225, 240, 243, 250, 256, 270, 288, 300, 320,
+          324, 360, 375, 384, 400, 405, 432, 450, 480, 486, 500, 512, 540, 576, 600, 625, 640, 648, 675, 720, 729,
+          750, 768, 800, 810, 864, 900, 960, 972, 1000, 1024>(rng);
   return 0;
 }

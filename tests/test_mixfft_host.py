@@ -30,7 +30,7 @@ def test_mixed_radix_fft_matches_fp64_dft(tmp_path):
                     str(HERE / "mixfft_host.cu"), "-o", str(exe)], check=True, capture_output=True, text=True)
     out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
     rows = [line.split() for line in out if line.strip()]
-    want = [n for n in range(6, 1001) if _smooth(n) and n & (n - 1)]
+    want = [n for n in range(4, 1025) if _smooth(n)]
     assert [int(r[0]) for r in rows] == want
     for n, a, b, fwd, inv, ea, eb in rows:
         assert int(a) * int(b) == int(n) and int(a) <= int(b)
