@@ -605,7 +605,8 @@ int coded_check(int n, int ds, const void* a, const void* b, const void* t2, con
     return set_error(PTX_ERR_WORKSPACE, "workspace of %zu bytes is smaller than the %zu bytes needed", ws_bytes,
                      fixed + per);
   }
-  g->chunk = static_cast<int>(std::min<size_t>((ws_bytes - fixed) / per, (size_t)std::max(batch, 1)));
+  // frames per chunk: what the workspace holds, at most the batch and 65535 (a grid dimension)
+  g->chunk = static_cast<int>(std::min<size_t>({(ws_bytes - fixed) / per, (size_t)std::max(batch, 1), (size_t)65535}));
   char* p = static_cast<char*>(ws) + kHdr;
   g->ospec = reinterpret_cast<float2*>(p);
   g->gospec = reinterpret_cast<float2*>(p + g->field_bytes);

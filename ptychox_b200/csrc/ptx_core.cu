@@ -113,9 +113,10 @@ int get_line_plan(int n, LinePlan* out) {
   p.nstages = make_radices(n, radix);
   p.radices = 0;
   for (int s = 0; s < p.nstages; ++s) p.radices |= static_cast<unsigned long long>(radix[s]) << (5 * s);
-  // the natural table (n entries), then for mixed-radix lengths the two layouts of the
-  // inter-step twiddles (n entries each)
-  const int mix_b = (n & (n - 1)) ? mix::split_b(n) : 0;
+  // the natural table (n entries), then the two layouts of the mixed-radix engine's
+  // inter-step twiddles (n entries each; every supported length has them: the generic-length
+  // FPM kernels run powers of two on that engine too)
+  const int mix_b = mix::split_b(n);
   const int entries = mix_b ? 3 * n : n;
   int offset;
   auto ot = g_table_offset.find(n);

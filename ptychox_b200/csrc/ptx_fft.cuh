@@ -28,9 +28,8 @@ struct LinePlan {
   int nstages;                // number of radix stages
   unsigned long long radices; // radix of stage s in bits [5s, 5s+5)
   const float2* tw;           // device table exp(-2 pi i m / n), m in [0, n)
-  // {2,3,5}-smooth lengths that are not powers of two, n = A * B (mix::Shape): the two
-  // layouts of exp(-2 pi i t u / n), t < B, u < A, mix_twt[u * B + t] = mix_twi[t * A + u]
-  // (null for other lengths)
+  // the mixed-radix engine's split n = A * B (mix::Shape): the two layouts of
+  // exp(-2 pi i t u / n), t < B, u < A, mix_twt[u * B + t] = mix_twi[t * A + u]
   const float2* mix_twt;
   const float2* mix_twi;
 };

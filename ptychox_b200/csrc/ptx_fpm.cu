@@ -15,7 +15,9 @@
 //   row pass   forward row DFT, /(h w), ifftshift placement, grad_S += Gl conj(pupil)
 //              (float2 atomics, with wrap), grad_pupil += Gl conj(S) in registers
 // S = fft2(O) before the frames and grad_O = n ifft2(grad_S) after them use the generic
-// 2-D passes.  All sides are powers of two (4..1024), so every modulo is a mask.
+// 2-D passes.  When all four sides are powers of two (4..1024) the kernels below run (every
+// modulo a mask); any other {2,3,5}-smooth sides take the mixed-radix kernels of
+// ptx_mixfpm.cuh through the same workspace layout.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -332,6 +334,8 @@ __global__ void __launch_bounds__(128, 3) fpm_rows_adjoint(
 struct FpmGeom {
   int oh, ow, lh, lw, batch;
   LinePlan p_ow, p_oh, p_lw, p_lh;
+  bool generic;  // a side is not a power of two: the mixed-radix kernels
+  const MixFpmOps *m_ow, *m_oh, *m_lw, *m_lh;
   size_t spec_bytes, tmp_bytes, frame_bytes;
   int chunk;
   float2* spec;   // workspace spectrum (sweep)
@@ -354,9 +358,10 @@ int fpm_check(const void* object, int oh, int ow, const void* pupil, int lh, int
   if (reinterpret_cast<uintptr_t>(ws) & 255) {
     return set_error(PTX_ERR_INVALID_ARGUMENT, "workspace must start on a 256-byte boundary");
   }
+  g->generic = !(is_pow2_len(oh) && is_pow2_len(ow) && is_pow2_len(lh) && is_pow2_len(lw));
   for (int n : {oh, ow, lh, lw}) {
-    if (!is_pow2_len(n)) {
-      return set_error(PTX_ERR_UNSUPPORTED_SIZE, "FPM sides must be powers of two in [4, 1024] (got %d)", n);
+    if (!(g->generic ? mix_fpm_ops(n) != nullptr : is_pow2_len(n))) {
+      return set_error(PTX_ERR_UNSUPPORTED_SIZE, "FPM sides must be 2^a 3^b 5^c in [4, 1024] (got %d)", n);
     }
   }
   if (lh > oh || lw > ow) return set_error(PTX_ERR_INVALID_ARGUMENT, "pupil larger than the object spectrum");
@@ -373,7 +378,10 @@ int fpm_check(const void* object, int oh, int ow, const void* pupil, int lh, int
     return set_error(PTX_ERR_WORKSPACE, "workspace of %zu bytes is smaller than the %zu bytes needed", ws_bytes,
                      fixed + g->frame_bytes);
   }
-  g->chunk = static_cast<int>(std::min<size_t>((ws_bytes - fixed) / g->frame_bytes, (size_t)std::max(batch, 1)));
+  // frames per chunk: what the workspace holds, at most the batch and 65535 (the column
+  // passes put the frame in gridDim.y)
+  g->chunk = static_cast<int>(
+      std::min<size_t>({(ws_bytes - fixed) / g->frame_bytes, (size_t)std::max(batch, 1), (size_t)65535}));
   g->lut = reinterpret_cast<float*>(static_cast<char*>(ws) + 256);
   char* p = static_cast<char*>(ws) + kHdr;
   g->spec = reinterpret_cast<float2*>(p);
@@ -381,6 +389,20 @@ int fpm_check(const void* object, int oh, int ow, const void* pupil, int lh, int
   g->tmp = reinterpret_cast<float2*>(p + 2 * g->spec_bytes);
   g->frames = reinterpret_cast<float2*>(p + 2 * g->spec_bytes + g->tmp_bytes);
   int st = PTX_OK;
+  if (g->generic) {
+    g->m_ow = mix_fpm_ops(ow);
+    g->m_oh = mix_fpm_ops(oh);
+    g->m_lw = mix_fpm_ops(lw);
+    g->m_lh = mix_fpm_ops(lh);
+    for (const LinePlan* p : {&g->p_ow, &g->p_oh, &g->p_lw, &g->p_lh}) {
+      if (!p->mix_twt) return set_error(PTX_ERR_UNSUPPORTED_SIZE, "no mixed-radix twiddle tables for length %d", p->n);
+    }
+    for (const MixFpmOps* o : {g->m_ow, g->m_oh, g->m_lw, g->m_lh}) {
+      if (!st) st = o->prepare();
+    }
+    return st;
+  }
+  g->m_ow = g->m_oh = g->m_lw = g->m_lh = nullptr;
   dispatch_pow2(ow, [&](auto NT) {
     constexpr int N = decltype(NT)::value;
     if (!st) st = ensure_smem((const void*)fft2_rows_kernel<N, false>, RowPass<N>::smem(RowPass<N>::lines(256, oh)));
@@ -407,10 +429,19 @@ int fpm_check(const void* object, int oh, int ow, const void* pupil, int lh, int
   return st;
 }
 
-// out = DFT2 (INV=false) or unnormalised inverse DFT2 (INV=true) of in, via tmp.
+// out = DFT2 (INV=false) or unnormalised inverse DFT2 (INV=true) of the H x W image in, via tmp.
 template <bool INV>
-void launch_fft2(const float2* in, int H, int W, float2* out, float scale, float2* tmp, const LinePlan& prow,
-                 const LinePlan& pcol, cudaStream_t s) {
+void launch_fft2(const FpmGeom& g, const float2* in, int H, int W, float2* out, float scale, float2* tmp,
+                 const LinePlan& prow, const LinePlan& pcol, cudaStream_t s) {
+  if (g.generic) {
+    prof_begin(kFft2Rows, s);
+    g.m_ow->fft2_rows(INV, in, H, tmp, prow.mix_twt, s);
+    prof_end(kFft2Rows, s);
+    prof_begin(kFft2Cols, s);
+    g.m_oh->fft2_cols(INV, tmp, W, out, scale, pcol.mix_twt, s);
+    prof_end(kFft2Cols, s);
+    return;
+  }
   prof_begin(kFft2Rows, s);
   dispatch_pow2(W, [&](auto NT) {
     constexpr int N = decltype(NT)::value;
@@ -432,6 +463,13 @@ void launch_fft2(const float2* in, int H, int W, float2* out, float scale, float
 void launch_rows_forward(const FpmGeom& g, const float2* spec, const float2* pupil, const int64_t* led, int nf,
                          cudaStream_t s) {
   prof_begin(kFpmRowsForward, s);
+  if (g.generic) {
+    MixFpmRowsArgs a{spec, g.oh, g.ow, pupil, g.lh, led, nf, g.frames, g.p_lw.mix_twt, g.p_lw.mix_twi, 0.f,
+                     nullptr, nullptr};
+    g.m_lw->rows_forward(a, s);
+    prof_end(kFpmRowsForward, s);
+    return;
+  }
   dispatch_pow2(g.lw, [&](auto NT) {
     constexpr int N = decltype(NT)::value;
     const int lines = RowPass<N>::lines(128, g.lh);
@@ -450,6 +488,13 @@ void launch_cols(const FpmGeom& g, int frame0, int nf, const uint16_t* measured,
                  cudaStream_t s) {
   const float norm = 1.0f / static_cast<float>((double)g.lh * g.lw);
   prof_begin(kFpmCols, s);
+  if (g.generic) {
+    MixFpmColsArgs a{g.frames, g.lw, frame0, nf, g.p_lh.mix_twt, g.p_lh.mix_twi, measured, g.lut, norm, grad_scale,
+                     inv_numel, loss, image, amplitude, grad_output};
+    g.m_lh->cols(MODE == kFpmSweep ? kMixColSweep : MODE == kFpmForward ? kMixColForward : kMixColBackward, a, s);
+    prof_end(kFpmCols, s);
+    return;
+  }
   dispatch_pow2(g.lh, [&](auto NT) {
     constexpr int N = decltype(NT)::value;
     if constexpr (MODE == kFpmSweep) {
@@ -476,6 +521,13 @@ void launch_rows_adjoint(const FpmGeom& g, const float2* spec, const float2* pup
                          float2* grad_spec, float2* grad_pupil, cudaStream_t s) {
   const float norm = 1.0f / static_cast<float>((double)g.lh * g.lw);
   prof_begin(kFpmRowsAdjoint, s);
+  if (g.generic) {
+    MixFpmRowsArgs a{spec, g.oh, g.ow, pupil, g.lh, led, nf, g.frames, g.p_lw.mix_twt, g.p_lw.mix_twi, norm,
+                     grad_spec, grad_pupil};
+    g.m_lw->rows_adjoint(a, s);
+    prof_end(kFpmRowsAdjoint, s);
+    return;
+  }
   dispatch_pow2(g.lw, [&](auto NT) {
     constexpr int N = decltype(NT)::value;
     const int lines = RowPass<N>::lines(128, g.lh);
@@ -513,7 +565,8 @@ int ptx_fpm_forward(const float* object, int object_h, int object_w, const float
   if (!spectrum || (!amplitude && batch > 0)) return set_error(PTX_ERR_INVALID_ARGUMENT, "null output");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   float2* spec = reinterpret_cast<float2*>(spectrum);
-  launch_fft2<false>(reinterpret_cast<const float2*>(object), object_h, object_w, spec, 1.0f, g.tmp, g.p_ow, g.p_oh, s);
+  launch_fft2<false>(g, reinterpret_cast<const float2*>(object), object_h, object_w, spec, 1.0f, g.tmp, g.p_ow, g.p_oh,
+                     s);
   const float2* P = reinterpret_cast<const float2*>(pupil);
   for (int b0 = 0; b0 < batch; b0 += g.chunk) {
     const int nf = std::min(g.chunk, batch - b0);
@@ -547,7 +600,7 @@ int ptx_fpm_backward(const float* grad_output, const float* image, const float* 
                               const_cast<float2*>(reinterpret_cast<const float2*>(image)), nullptr, grad_output, s);
     launch_rows_adjoint(g, spec, P, led_indices_xy + 2 * (size_t)b0, nf, g.gspec, GP, s);
   }
-  launch_fft2<true>(g.gspec, object_h, object_w, reinterpret_cast<float2*>(grad_object), 1.0f, g.tmp, g.p_ow, g.p_oh,
+  launch_fft2<true>(g, g.gspec, object_h, object_w, reinterpret_cast<float2*>(grad_object), 1.0f, g.tmp, g.p_ow, g.p_oh,
                     s);
   return cuda_status(cudaGetLastError(), "ptx_fpm_backward launch");
 }
@@ -574,7 +627,7 @@ int ptx_fpm_sweep(const float* object, int object_h, int object_w, const float* 
         g.gspec, ns, reinterpret_cast<float2*>(grad_pupil), np, loss, nullptr, g.lut, scale);
     prof_end(kMiscKernel, s);
   }
-  launch_fft2<false>(reinterpret_cast<const float2*>(object), object_h, object_w, g.spec, 1.0f, g.tmp, g.p_ow, g.p_oh,
+  launch_fft2<false>(g, reinterpret_cast<const float2*>(object), object_h, object_w, g.spec, 1.0f, g.tmp, g.p_ow, g.p_oh,
                      s);
   const float2* P = reinterpret_cast<const float2*>(pupil);
   float2* GP = reinterpret_cast<float2*>(grad_pupil);
@@ -586,7 +639,7 @@ int ptx_fpm_sweep(const float* object, int object_h, int object_w, const float* 
                            nullptr, s);
     launch_rows_adjoint(g, g.spec, P, led, nf, g.gspec, GP, s);
   }
-  launch_fft2<true>(g.gspec, object_h, object_w, reinterpret_cast<float2*>(grad_object), 1.0f, g.tmp, g.p_ow, g.p_oh,
+  launch_fft2<true>(g, g.gspec, object_h, object_w, reinterpret_cast<float2*>(grad_object), 1.0f, g.tmp, g.p_ow, g.p_oh,
                     s);
   return cuda_status(cudaGetLastError(), "ptx_fpm_sweep launch");
 }

@@ -169,4 +169,49 @@ struct MixOps {
 };
 const MixOps* mix_ops(int n);
 
+// ---- Fourier ptychography on the mixed-radix engine (ptx_mixfpm.cuh) -------------------
+// Used when any of the four FPM sides is not a power of two; compiled for every
+// {2,3,5}-smooth length 4..1024 (mix_fpm_ops(n) is null for every other length).
+struct MixFpmRowsArgs {
+  const float2* spec;   // object spectrum, oh x ow
+  int oh, ow;
+  const float2* pupil;  // lh x lw
+  int lh;
+  const int64_t* led;   // (x, y) window corner of each frame in the shifted spectrum
+  int nframes;
+  float2* scratch;      // tiled frames [frame][tile][row][16], lh x lw
+  const float2* twt;    // row-length (lw) twiddles
+  const float2* twi;
+  float norm;           // 1 / (lh lw) (adjoint)
+  float2* grad_spec;    // adjoint outputs (float2 atomics)
+  float2* grad_pupil;
+};
+struct MixFpmColsArgs {
+  float2* scratch;
+  int lw, frame0, nframes;
+  const float2* twt;  // column-length (lh) twiddles
+  const float2* twi;
+  const uint16_t* measured;  // sweep: counts (not shifted)
+  const float* lut;
+  float norm;                // 1 / (lh lw)
+  float grad_scale;
+  double inv_numel;
+  double* loss;
+  float2* image;             // forward: optional output; backward: input
+  float* amplitude;          // forward output
+  const float* grad_output;  // backward input
+};
+struct MixFpmOps {
+  int (*prepare)();
+  // one image: rows (natural [H][n] -> tiled [tiles(n)][H][16]) and columns (tiled
+  // [tiles(W)][n][16] -> natural [n][W] times `scale`); plus: exp(+i) (unnormalised inverse)
+  void (*fft2_rows)(bool plus, const float2* in, int H, float2* tiled, const float2* twt, cudaStream_t);
+  void (*fft2_cols)(bool plus, const float2* tiled, int W, float2* out, float scale, const float2* twt,
+                    cudaStream_t);
+  void (*rows_forward)(const MixFpmRowsArgs&, cudaStream_t);
+  void (*rows_adjoint)(const MixFpmRowsArgs&, cudaStream_t);
+  void (*cols)(int mode, const MixFpmColsArgs&, cudaStream_t);
+};
+const MixFpmOps* mix_fpm_ops(int n);
+
 }  // namespace ptx

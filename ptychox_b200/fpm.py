@@ -3,8 +3,9 @@
 Drop-in for ``python/ptychoX/fpm/ops.py``: ``ptychoX_fourier`` / ``fourier_ptychography``
 keep the reference signature (:14-25) and ``autograd.Function`` contract (:37-99).  The
 forward saves the object spectrum ``fft2(O)`` (``[H, W]``) instead of the reference's
-``[B, h, w]`` sub-spectrum stack; the backward re-gathers the windows from it.  All sides
-must be powers of two in [4, 1024].  ``ptychoX_fourier_loss`` is the fused sweep.
+``[B, h, w]`` sub-spectrum stack; the backward re-gathers the windows from it.  Sides are
+2^a 3^b 5^c in [4, 1024] (the reference's cuFFT takes any side; other lengths raise
+``ValueError``).  ``ptychoX_fourier_loss`` is the fused sweep.
 """
 
 from __future__ import annotations
