@@ -129,5 +129,7 @@ def test_rectangular_and_unsupported():
     amp = ptychoX_fourier(cuda(obj), cuda(pup), cuda(led))
     ramp, _, _ = O.fpm_forward(obj, pup, led)
     assert rel_l2(amp.cpu().numpy(), ramp) < TOL
+    amp96 = ptychoX_fourier(cuda(obj[:, :96]), cuda(pup), cuda(led))  # 96 = 2^5 3: the mixed-radix path
+    assert rel_l2(amp96.cpu().numpy(), O.fpm_forward(obj[:, :96], pup, led)[0]) < TOL
     with pytest.raises(ValueError):
-        ptychoX_fourier(cuda(obj[:, :96]), cuda(pup), cuda(led))  # 96 is not a power of two
+        ptychoX_fourier(cuda(obj[:, :112]), cuda(pup), cuda(led))  # 112 = 2^4 7: no FFT length
