@@ -450,10 +450,11 @@ def serving_mix(n_requests: int, seed: int = 0, rate: float = 20.0) -> list[tupl
     LEDs, 1024^2 spectrum), coded / near-field (1024^2 field, 64 shifts, ds 4) and the
     conventional large scan (512^2 probe, 30x30 raster), sizes jittered by U[0.75, 1.25]:
     conventional probe sides snapped to the nearest 2^a 3^b 5^c length (96..640: lengths
-    such as 100, 120, 144, 160, 480, 600 run on the runtime-plan FFT kernels), scan grids
-    jittered with positions held in [49, 900], Fourier LED grids and coded shift counts
-    jittered; the Fourier and coded sides stay powers of two (their kernels are the
-    power-of-two register FFT, and 1024 / 256 are the only powers of two within 25%).
+    such as 100, 120, 144, 160, 480, 600 run on the mixed-radix register FFT), scan grids
+    jittered with positions held in [49, 900]; Fourier pupil sides snapped likewise
+    (192..320) in a spectrum of the largest smooth side up to min(1024, 4 h), LED grids
+    jittered; coded / near-field shift counts jittered, their fields stay 1024^2 (the coded
+    kernels are the power-of-two register FFT, and 1024 is the only power of two within 25%).
     """
     rng = np.random.default_rng(seed)
     t = 0.0
@@ -473,7 +474,9 @@ def serving_mix(n_requests: int, seed: int = 0, rate: float = 20.0) -> list[tupl
             out.append((rid, "conventional", t, {"p": p, "grid": grid, "step": step, "n": n}))
         elif u < 0.7:
             grid = int(min(15, max(7, round(15 * j()))))
-            out.append((rid, "fourier", t, {"n": 1024, "h": 256, "grid": grid}))
+            h = snap_smooth(256 * j())
+            n = max(m for m in _SMOOTH if m <= min(1024, 4 * h))
+            out.append((rid, "fourier", t, {"n": n, "h": h, "grid": grid}))
         else:
             count = int(max(16, round(64 * j())))
             out.append((rid, "coded" if rng.uniform() < 0.5 else "nearfield", t, {"n": 1024, "count": count, "ds": 4}))
