@@ -8,8 +8,10 @@ used; here the hand-written adjoint always runs (it equals autograd's product).
 
 ``ptychoX_nearfield(object_field, probe_field, transfer, shifts_xy, downsample)`` is the
 near-field operator of the MATLAB class ``adPtychoX_nearf`` = coded with
-``transfer_1 = 1``.  Fields are square with a power-of-two side in [16, 1024];
-``downsample`` must divide the side and 8.
+``transfer_1 = 1``.  Fields are square with a 2^a 3^b 5^c side in [16, 1024] (the
+reference's cuFFT takes any side; other sides raise ``ValueError``); ``downsample`` must
+divide the side (and, for power-of-two sides, the row group of 8, for others a row group of
+at most 512 threads).
 """
 
 from __future__ import annotations

@@ -22,7 +22,9 @@
 //   7 col: forward column DFT, /n, grad_O^ += . conj(T1 R_b) (float2 atomics)
 // O^ = D(O) before the frames and grad_O = D*(grad_O^) after them use the generic 2-D
 // passes.  The phase ramp's argument is reduced exactly in FP32 (FMA two-product and
-// integer rounding) before sincospif, so the ramp is accurate to ~1 ulp of a turn.
+// integer rounding) before sincospif, so the ramp is accurate to ~1 ulp of a turn.  Field
+// sides that are {2,3,5}-smooth but not powers of two run the same passes on the mixed-radix
+// kernels of ptx_mixcoded.cuh through the same workspace layout.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -562,6 +564,8 @@ __global__ void __launch_bounds__(256) fd_loss_kernel(const float* __restrict__ 
 struct CodedGeom {
   int n, ds, batch;
   LinePlan plan;
+  const MixCodedOps* mix;  // non-null: the mixed-radix passes (side not a power of two)
+  const MixFpmOps* mfft;   // their 2-D transforms of the object spectrum
   size_t field_bytes;
   int chunk;
   float2* ospec;
@@ -571,7 +575,12 @@ struct CodedGeom {
   float2* frames;
 };
 
-size_t coded_fixed_bytes(int n) { return kHdr + 3 * (size_t)n * n * sizeof(float2); }
+// A field n x n in natural layout, and one in the tiled frame layout [tile][row][16] (the
+// same when 16 divides n).
+size_t field_bytes_of(int n) { return (size_t)n * n * sizeof(float2); }
+size_t tiled_bytes_of(int n) { return (size_t)num_tiles(n) * kTile * n * sizeof(float2); }
+// object spectrum and its gradient (natural), the 2-D transforms' temporary (tiled)
+size_t coded_fixed_bytes(int n) { return kHdr + 2 * field_bytes_of(n) + tiled_bytes_of(n); }
 
 int coded_lines(int n) {
   int lines = 0;
@@ -589,18 +598,27 @@ int coded_check(int n, int ds, const void* a, const void* b, const void* t2, con
   if (reinterpret_cast<uintptr_t>(ws) & 255) {
     return set_error(PTX_ERR_INVALID_ARGUMENT, "workspace must start on a 256-byte boundary");
   }
-  if (!is_pow2_len(n) || n < 16) {
-    return set_error(PTX_ERR_UNSUPPORTED_SIZE, "coded field side must be a power of two in [16, 1024] (got %d)", n);
+  const bool pow2 = is_pow2_len(n) && n >= 16;
+  g->mix = pow2 ? nullptr : mix_coded_ops(n);
+  g->mfft = pow2 ? nullptr : mix_fpm_ops(n);
+  if (!pow2 && !(g->mix && g->mfft)) {
+    return set_error(PTX_ERR_UNSUPPORTED_SIZE, "coded field side must be 2^a 3^b 5^c in [16, 1024] (got %d)", n);
   }
-  const int lines = coded_lines(n);
-  if (ds < 1 || n % ds != 0 || lines % ds != 0) {
-    return set_error(PTX_ERR_UNSUPPORTED_SIZE, "downsample %d must divide %d and %d", ds, n, lines);
+  if (pow2) {
+    const int lines = coded_lines(n);
+    if (ds < 1 || n % ds != 0 || lines % ds != 0) {
+      return set_error(PTX_ERR_UNSUPPORTED_SIZE, "downsample %d must divide %d and %d", ds, n, lines);
+    }
+  } else if (ds < 1 || n % ds != 0) {
+    return set_error(PTX_ERR_UNSUPPORTED_SIZE, "downsample %d must divide %d", ds, n);
   }
   g->n = n; g->ds = ds; g->batch = batch;
   if (int st = get_line_plan(n, &g->plan)) return st;
-  g->field_bytes = (size_t)n * n * sizeof(float2);
+  if (!pow2 && !g->plan.mix_twt) return set_error(PTX_ERR_UNSUPPORTED_SIZE, "no mixed-radix twiddle tables for %d", n);
+  g->field_bytes = field_bytes_of(n);
+  const size_t tiled = tiled_bytes_of(n);
   const size_t fixed = coded_fixed_bytes(n);
-  const size_t per = g->field_bytes * (need_xstore ? 2 : 1);
+  const size_t per = tiled + (need_xstore ? g->field_bytes : 0);  // a frame and its stored x
   if (ws_bytes < fixed + per) {
     return set_error(PTX_ERR_WORKSPACE, "workspace of %zu bytes is smaller than the %zu bytes needed", ws_bytes,
                      fixed + per);
@@ -611,9 +629,15 @@ int coded_check(int n, int ds, const void* a, const void* b, const void* t2, con
   g->ospec = reinterpret_cast<float2*>(p);
   g->gospec = reinterpret_cast<float2*>(p + g->field_bytes);
   g->tmp = reinterpret_cast<float2*>(p + 2 * g->field_bytes);
-  g->frames = reinterpret_cast<float2*>(p + 3 * g->field_bytes);
-  g->xstore = need_xstore ? reinterpret_cast<float2*>(p + 3 * g->field_bytes + (size_t)g->chunk * g->field_bytes)
+  g->frames = reinterpret_cast<float2*>(p + 2 * g->field_bytes + tiled);
+  g->xstore = need_xstore ? reinterpret_cast<float2*>(p + 2 * g->field_bytes + tiled + (size_t)g->chunk * tiled)
                           : nullptr;
+  if (g->mix) {
+    int st = g->mix->prepare(ds);
+    if (!st) st = g->mfft->prepare();
+    return st;
+  }
+  const int lines = coded_lines(n);
   int st = PTX_OK;
   dispatch_pow2(n, [&](auto NT) {
     constexpr int N = decltype(NT)::value;
@@ -640,8 +664,32 @@ int coded_check(int n, int ds, const void* a, const void* b, const void* t2, con
   return st;
 }
 
+// Arguments of the mixed-radix passes common to all of them; callers fill in the rest.
+MixCodedArgs mix_args(const CodedGeom& g, int nf, float inv_n) {
+  MixCodedArgs a{};
+  a.scratch = g.frames;
+  a.ospec = g.ospec;
+  a.inv_n = inv_n;
+  a.grad_ospec = g.gospec;
+  a.twt = g.plan.mix_twt;
+  a.twi = g.plan.mix_twi;
+  a.ds = g.ds;
+  a.nframes = nf;
+  return a;
+}
+
 template <bool INV>
-void launch_fft2(const float2* in, int n, float2* out, float2* tmp, const LinePlan& p, cudaStream_t s) {
+void launch_fft2(const CodedGeom& g, const float2* in, int n, float2* out, float2* tmp, const LinePlan& p,
+                 cudaStream_t s) {
+  if (g.mix) {
+    prof_begin(kFft2Rows, s);
+    g.mfft->fft2_rows(INV, in, n, tmp, p.mix_twt, s);
+    prof_end(kFft2Rows, s);
+    prof_begin(kFft2Cols, s);
+    g.mfft->fft2_cols(INV, tmp, n, out, 1.0f, p.mix_twt, s);
+    prof_end(kFft2Cols, s);
+    return;
+  }
   dispatch_pow2(n, [&](auto NT) {
     constexpr int N = decltype(NT)::value;
     const int lines = RowPass<N>::lines(256, N);
@@ -661,6 +709,16 @@ void launch_cols(const CodedGeom& g, int nf, const float2* t1, const float2* t2,
                  cudaStream_t s, double* grad_shifts = nullptr) {
   const float inv_n = 1.0f / static_cast<float>((double)g.n * g.n);
   prof_begin(kCodedCols, s);
+  if (g.mix) {
+    MixCodedArgs a = mix_args(g, nf, inv_n);
+    a.t1 = t1;
+    a.t2 = t2;
+    a.shifts = shifts;
+    a.grad_shifts = STAGE == 7 ? grad_shifts : nullptr;
+    g.mix->cols(STAGE, CONJ, a, s);
+    prof_end(kCodedCols, s);
+    return;
+  }
   dispatch_pow2(g.n, [&](auto NT) {
     constexpr int N = decltype(NT)::value;
     if constexpr (STAGE == 3) {
@@ -683,6 +741,14 @@ void launch_cols(const CodedGeom& g, int nf, const float2* t1, const float2* t2,
 void launch_rows_mask(const CodedGeom& g, int nf, const float2* mask, float2* xstore, cudaStream_t s) {
   const float inv_n = 1.0f / static_cast<float>((double)g.n * g.n);
   prof_begin(kCodedRows, s);
+  if (g.mix) {
+    MixCodedArgs a = mix_args(g, nf, inv_n);
+    a.mask = mask;
+    a.xstore = xstore;
+    g.mix->rows_mask(a, s);
+    prof_end(kCodedRows, s);
+    return;
+  }
   dispatch_pow2(g.n, [&](auto NT) {
     constexpr int N = decltype(NT)::value;
     const int lines = RowPass<N>::lines(128, N);
@@ -700,6 +766,22 @@ void launch_rows_pool(const CodedGeom& g, int frame0, int nf, const uint16_t* me
                       const float* grad_output, cudaStream_t s) {
   const float inv_n = 1.0f / static_cast<float>((double)g.n * g.n);
   prof_begin(kCodedRows, s);
+  if (g.mix) {
+    MixCodedArgs a = mix_args(g, nf, inv_n);
+    a.frame0 = frame0;
+    a.measured = measured;
+    a.scale = scale;
+    a.grad_scale = grad_scale;
+    a.inv_numel = inv_numel;
+    a.loss = loss;
+    a.sensor = sensor;
+    a.amplitude = amplitude;
+    a.grad_output = grad_output;
+    g.mix->rows_pool(MODE == kCodedSweep ? kMixColSweep : MODE == kCodedForward ? kMixColForward : kMixColBackward,
+                     a, s);
+    prof_end(kCodedRows, s);
+    return;
+  }
   dispatch_pow2(g.n, [&](auto NT) {
     constexpr int N = decltype(NT)::value;
     const int lines = RowPass<N>::lines(256, N);
@@ -715,6 +797,15 @@ void launch_rows_pool(const CodedGeom& g, int frame0, int nf, const uint16_t* me
 void launch_rows_grad_mask(const CodedGeom& g, int nf, const float2* mask, const float2* xstore, float2* grad_mask,
                            cudaStream_t s) {
   prof_begin(kCodedRows, s);
+  if (g.mix) {
+    MixCodedArgs a = mix_args(g, nf, 1.0f / static_cast<float>((double)g.n * g.n));
+    a.mask = mask;
+    a.xstore = const_cast<float2*>(xstore);
+    a.grad_mask = grad_mask;
+    g.mix->rows_grad_mask(a, s);
+    prof_end(kCodedRows, s);
+    return;
+  }
   dispatch_pow2(g.n, [&](auto NT) {
     constexpr int N = decltype(NT)::value;
     const int lines = RowPass<N>::lines(128, N);
@@ -773,7 +864,7 @@ int coded_backward_impl(const float* grad_output, const float* x_forward, const 
                  reinterpret_cast<const float2*>(x_forward) + (size_t)b0 * n * n,
                  reinterpret_cast<float2*>(grad_coded), s, grad_shifts ? grad_shifts + 2 * (size_t)b0 : nullptr);
   }
-  launch_fft2<true>(g.gospec, n, reinterpret_cast<float2*>(grad_object), g.tmp, g.plan, s);
+  launch_fft2<true>(g, g.gospec, n, reinterpret_cast<float2*>(grad_object), g.tmp, g.plan, s);
   return cuda_status(cudaGetLastError(), "ptx_coded_backward launch");
 }
 
@@ -784,9 +875,9 @@ extern "C" {
 
 size_t ptx_coded_workspace_bytes(int n, int batch) {
   if (n <= 0) return 0;
-  const size_t field = (size_t)n * n * sizeof(float2);
-  const size_t frames = std::max<size_t>(1, std::min<size_t>((size_t)std::max(batch, 1), (4096ull << 20) / (2 * field)));
-  return coded_fixed_bytes(n) + frames * 2 * field;
+  const size_t per = tiled_bytes_of(n) + field_bytes_of(n);  // a frame and its stored x
+  const size_t frames = std::max<size_t>(1, std::min<size_t>((size_t)std::max(batch, 1), (4096ull << 20) / per));
+  return coded_fixed_bytes(n) + frames * per;
 }
 
 int ptx_coded_forward(const float* object, const float* coded_surface, const float* transfer_1, const float* transfer_2,
@@ -802,7 +893,7 @@ int ptx_coded_forward(const float* object, const float* coded_surface, const flo
   const float2* T1 = reinterpret_cast<const float2*>(transfer_1);
   const float2* T2 = reinterpret_cast<const float2*>(transfer_2);
   const float2* M = reinterpret_cast<const float2*>(coded_surface);
-  launch_fft2<false>(reinterpret_cast<const float2*>(object), n, g.ospec, g.tmp, g.plan, s);
+  launch_fft2<false>(g, reinterpret_cast<const float2*>(object), n, g.ospec, g.tmp, g.plan, s);
   for (int b0 = 0; b0 < batch; b0 += g.chunk) {
     const int nf = std::min(g.chunk, batch - b0);
     const float* sh = shifts_xy + 2 * (size_t)b0;
@@ -852,7 +943,7 @@ static int coded_sweep_mse(const float* object, const float* coded_surface, cons
   const int lw = n / downsample;
   const double numel = (double)batch * lw * lw;
   const float grad_scale = static_cast<float>(2.0 / std::max(numel, 1.0));
-  launch_fft2<false>(reinterpret_cast<const float2*>(object), n, g.ospec, g.tmp, g.plan, s);
+  launch_fft2<false>(g, reinterpret_cast<const float2*>(object), n, g.ospec, g.tmp, g.plan, s);
   for (int b0 = 0; b0 < batch; b0 += g.chunk) {
     const int nf = std::min(g.chunk, batch - b0);
     const float* sh = shifts_xy + 2 * (size_t)b0;
@@ -864,7 +955,7 @@ static int coded_sweep_mse(const float* object, const float* coded_surface, cons
     adjoint_tail(g, nf, M, T1, T2, sh, g.xstore, reinterpret_cast<float2*>(grad_coded), s,
                  grad_shifts ? grad_shifts + 2 * (size_t)b0 : nullptr);
   }
-  launch_fft2<true>(g.gospec, n, reinterpret_cast<float2*>(grad_object), g.tmp, g.plan, s);
+  launch_fft2<true>(g, g.gospec, n, reinterpret_cast<float2*>(grad_object), g.tmp, g.plan, s);
   return cuda_status(cudaGetLastError(), "ptx_coded_sweep launch");
 }
 

@@ -214,4 +214,39 @@ struct MixFpmOps {
 };
 const MixFpmOps* mix_fpm_ops(int n);
 
+// ---- coded / near-field on the mixed-radix engine (ptx_mixcoded.cuh) --------------------
+// Field sides that are {2,3,5}-smooth but not powers of two, 16..1000 (mix_coded_ops(n) is
+// null for every other side).
+struct MixCodedArgs {
+  float2* scratch;          // tiled frames [frame][tile][row][16], n x n
+  const float2* ospec;      // O^ = fft2(O)
+  const float2* t1;         // first transfer function (null: near-field)
+  const float2* t2;
+  const float* shifts;      // (dx, dy) per frame of this chunk
+  float inv_n;              // 1 / n^2
+  float2* grad_ospec;
+  const float2* twt;        // line twiddles of n (LinePlan::mix_twt / mix_twi)
+  const float2* twi;
+  double* grad_shifts;      // pass 7, optional
+  const float2* mask;       // coded surface M
+  float2* xstore;           // x = ifft2(O^ T1 R) per frame of this chunk
+  float2* grad_mask;
+  int ds, frame0, nframes;
+  const uint16_t* measured;  // pass 4 (sweep)
+  float scale, grad_scale;
+  double inv_numel;
+  double* loss;
+  float2* sensor;            // pass 4: forward output / backward input
+  float* amplitude;
+  const float* grad_output;
+};
+struct MixCodedOps {
+  int (*prepare)(int ds);  // also rejects a downsample whose row group does not fit a CTA
+  void (*cols)(int stage, bool conj, const MixCodedArgs&, cudaStream_t);  // passes 1, 3 / 5, 7
+  void (*rows_mask)(const MixCodedArgs&, cudaStream_t);                   // pass 2
+  void (*rows_pool)(int mode, const MixCodedArgs&, cudaStream_t);         // pass 4 (MixColMode)
+  void (*rows_grad_mask)(const MixCodedArgs&, cudaStream_t);              // pass 6
+};
+const MixCodedOps* mix_coded_ops(int n);
+
 }  // namespace ptx

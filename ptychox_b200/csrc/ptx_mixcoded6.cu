@@ -1,0 +1,19 @@
+// Mixed-radix coded / near-field kernels, length group 6 (ptx_mix_lengths.h).
+#include "ptx_mix_lengths.h"
+#include "ptx_mixcoded.cuh"
+
+namespace ptx {
+
+const MixCodedOps* mix_coded_ops_group6(int n) {
+#define PTX_MIXCODED_CASE(N) \
+  case N:                    \
+    return mixcoded::Ops<N>::table();
+  switch (n) {
+    PTX_MIXCODED_GROUP6(PTX_MIXCODED_CASE)
+    default:
+      return nullptr;
+  }
+#undef PTX_MIXCODED_CASE
+}
+
+}  // namespace ptx

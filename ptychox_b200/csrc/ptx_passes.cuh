@@ -126,8 +126,9 @@ __device__ __forceinline__ void abs_and_inv(float2 z, float eps, float& a, float
 }
 
 // Sum a per-thread FP64 partial over the block and add it (times `scale`) to *out.
-// Every thread of the block must call it; blocks smaller than a warp take the
-// shared-memory atomic route (a full-mask shuffle needs all 32 lanes).
+// Every thread of the block must call it; blocks that are not whole warps take the
+// shared-memory atomic route (a full-mask shuffle needs all 32 lanes).  Calls may follow one
+// another (the staging array is free again when a call returns).
 __device__ __forceinline__ void block_add_double(double v, double scale, double* out) {
   __shared__ double red[32];
   const int tid = threadIdx.x;
@@ -143,6 +144,7 @@ __device__ __forceinline__ void block_add_double(double v, double scale, double*
       for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
       if (tid == 0) atomicAdd(out, w * scale);
     }
+    __syncthreads();  // red is read: a following call may write it
   } else {
     if (tid == 0) red[0] = 0.0;
     __syncthreads();

@@ -126,9 +126,9 @@ def test_input_errors():
         ptychoX_coded(z, z, z, z, sh, 3)
     with pytest.raises(ValueError, match=r"shape \[batch, 2\]"):
         ptychoX_coded(z, z, z, z, sh[:, :1], 2)
-    w = torch.zeros(96, 96, dtype=torch.complex64, device="cuda")
+    w = torch.zeros(112, 112, dtype=torch.complex64, device="cuda")
     with pytest.raises(ValueError):
-        ptychoX_coded(w, w, w, w, sh, 2)  # 96 is not a power of two
+        ptychoX_coded(w, w, w, w, sh, 2)  # 112 = 2^4 7: no FFT length
 
 
 @pytest.mark.parametrize("name,loss", [("sweep_coded_fd_iso_fp64.npz", "fd-isotropic"),
