@@ -165,7 +165,9 @@ int get_line_plan(int n, LinePlan* out) {
 }
 
 int ensure_smem(const void* kernel, int bytes) {
-  if (bytes <= 48 * 1024) return PTX_OK;
+  // the default 48 KB cap covers a kernel's static shared memory too (block reductions
+  // keep up to a few hundred bytes there): raise the cap for anything within 1 KB of it
+  if (bytes + 1024 <= 48 * 1024) return PTX_OK;
   return cuda_status(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
                      "cudaFuncSetAttribute(MaxDynamicSharedMemorySize)");
 }

@@ -23,7 +23,8 @@ int cuda_status(cudaError_t e, const char* what);
 int get_line_plan(int n, LinePlan* out);
 bool size_supported(int n);
 
-// Enable large dynamic shared memory on a kernel once per device.
+// Raise a kernel's dynamic shared memory cap to `bytes` when they come near the 48 KB default
+// (which static shared memory also counts against).
 int ensure_smem(const void* kernel, int bytes);
 
 inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
@@ -113,8 +114,9 @@ bool dispatch_pow2(int n, F&& f) {
 }
 inline bool is_pow2_len(int n) { return n >= 4 && n <= 1024 && (n & (n - 1)) == 0; }
 
-// Line lengths that get compile-time FFT plans; every other supported length runs the
-// runtime-plan kernels (template argument 0).
+// Power-of-two line lengths with compile-time register FFT kernels in the conventional
+// passes; every other length gets template argument 0 (the mixed-radix kernels where
+// mix_ops(n) is non-null, else the runtime-plan kernels).
 template <typename F>
 void dispatch_len(int n, F&& f) {
   switch (n) {
