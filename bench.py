@@ -358,12 +358,15 @@ WORKLOADS = {
         Conventional("conventional-900x512-2048", 2048, 512, 30, 48, 64, 3, 1e5),
         Conventional("conventional-121x128-512", 512, 128, 11, 32, 8, 2, 1e4),
         ConventionalSubpixel("conventional-subpixel-900x512-2048", 2048, 512, 30, 48, 64, 3, 1e5),
-        # {2,3,5}-smooth probe sides of the serving mix's range, on the runtime-plan FFT kernels
+        # {2,3,5}-smooth probe sides of the serving mix's range, on the mixed-radix FFT kernels
         Conventional("conventional-121x96-512", 512, 96, 11, 32, 8, 2, 1e4),
         Conventional("conventional-121x160-640", 640, 160, 11, 40, 8, 2, 1e4),
         Conventional("conventional-400x640-2048", 2048, 640, 20, 64, 64, 3, 1e5),
         Fourier("fourier-225x256-1024", 1024, 256, 15, 5e3),
+        # config 2 and 3 geometry at smooth sides that are not powers of two (mixed-radix kernels)
+        Fourier("fourier-169x240-960", 960, 240, 13, 5e3),
         Coded("coded-64x1024-ds4", 1024, 64, 4, 2e3, nearfield=False),
+        Coded("coded-64x960-ds4", 960, 64, 4, 2e3, nearfield=False),
         Coded("nearfield-64x1024-ds4", 1024, 64, 4, 2e3, nearfield=True),
         Coded("coded-fd-64x1024-ds4", 1024, 64, 4, 2e3, nearfield=False, loss="fd-isotropic"),
     ]

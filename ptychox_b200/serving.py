@@ -453,8 +453,9 @@ def serving_mix(n_requests: int, seed: int = 0, rate: float = 20.0) -> list[tupl
     such as 100, 120, 144, 160, 480, 600 run on the mixed-radix register FFT), scan grids
     jittered with positions held in [49, 900]; Fourier pupil sides snapped likewise
     (192..320) in a spectrum of the largest smooth side up to min(1024, 4 h), LED grids
-    jittered; coded / near-field shift counts jittered, their fields stay 1024^2 (the coded
-    kernels are the power-of-two register FFT, and 1024 is the only power of two within 25%).
+    jittered; coded / near-field fields snapped to the nearest smooth side in [768, 1024] that
+    the downsampling factor 4 divides (768, 800, 864, 900, 960, 972, 1000, 1024), shift counts
+    jittered.
     """
     rng = np.random.default_rng(seed)
     t = 0.0
@@ -479,5 +480,7 @@ def serving_mix(n_requests: int, seed: int = 0, rate: float = 20.0) -> list[tupl
             out.append((rid, "fourier", t, {"n": n, "h": h, "grid": grid}))
         else:
             count = int(max(16, round(64 * j())))
-            out.append((rid, "coded" if rng.uniform() < 0.5 else "nearfield", t, {"n": 1024, "count": count, "ds": 4}))
+            n0 = 1024 * j()
+            n = min((m for m in _SMOOTH if 768 <= m <= 1024 and m % 4 == 0), key=lambda m: (abs(m - n0), m))
+            out.append((rid, "coded" if rng.uniform() < 0.5 else "nearfield", t, {"n": n, "count": count, "ds": 4}))
     return out
