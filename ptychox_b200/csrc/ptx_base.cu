@@ -277,6 +277,7 @@ __global__ void __launch_bounds__(128, 3) base_rows_forward_reg(
     const float2* __restrict__ sample, int H, int W, const float2* __restrict__ probe, int ph,
     const int64_t* __restrict__ pos, int nframes, int rowgroups, float2* __restrict__ scratch,
     const float2* __restrict__ tw, int lines, unsigned* __restrict__ err) {
+  pdl_wait();
   using S = RegShape<N>;
   using Cfg = FwdCfg<N>;
   constexpr int kTiles = N / kTile;
@@ -516,6 +517,7 @@ __global__ void __launch_bounds__(128, 2) base_rows_adjoint_reg(
     const float2* __restrict__ scratch, const float2* __restrict__ sample, int H, int W,
     const float2* __restrict__ probe, int ph, const int64_t* __restrict__ pos, int nframes, int rowgroups,
     float2* __restrict__ grad_sample, float2* __restrict__ grad_probe, const float2* __restrict__ tw, int lines) {
+  pdl_wait();
   using S = RegShape<N>;
   using Cfg = AdjCfg<N>;
   constexpr int kTiles = N / kTile;
@@ -660,6 +662,7 @@ __global__ void __launch_bounds__(256, 1) base_sweep_frame(
     const float* __restrict__ lut, float grad_scale, double inv_numel, double* __restrict__ loss,
     float2* __restrict__ grad_sample, float2* __restrict__ grad_probe, const float2* __restrict__ tw,
     unsigned* __restrict__ err) {
+  pdl_wait();
   using S = RegShape<N>;
   using Cfg = FrameCfg<N>;
   extern __shared__ float2 sm[];
@@ -856,7 +859,7 @@ void launch_rows_forward(const BaseGeom& g, const float2* sample, const float2* 
       const int rowgroups = (g.ph + lines - 1) / lines;
       const int threads = lines * L::T, smem = FwdCfg<N>::smem(lines);
       const int grid = persistent_grid((const void*)base_rows_forward_reg<N>, threads, smem, (long long)rowgroups * nframes);
-      base_rows_forward_reg<N><<<grid, threads, smem, s>>>(sample, g.H, g.W, probe, g.ph, pos, nframes, rowgroups,
+      launch_pdl(base_rows_forward_reg<N>, grid, threads, smem, s, sample, g.H, g.W, probe, g.ph, pos, nframes, rowgroups,
                                                            g.scratch, g.row.tw, lines, g.err);
     } else if (const MixOps* mo = mix_ops(g.pw)) {
       MixRowsArgs a{sample, g.H, g.W, probe, g.ph, g.pw, pos, nframes, g.scratch, g.row.mix_twt, g.row.mix_twi,
@@ -884,7 +887,7 @@ void launch_rows_adjoint(const BaseGeom& g, const float2* sample, const float2* 
       const int threads = lines * L::T, smem = L::adj_smem(lines);
       const long long units = (long long)rowgroups * nframes;
       const int grid = persistent_grid((const void*)base_rows_adjoint_reg<N>, threads, smem, units);
-      base_rows_adjoint_reg<N><<<grid, threads, smem, s>>>(g.scratch, sample, g.H, g.W, probe, g.ph, pos, nframes,
+      launch_pdl(base_rows_adjoint_reg<N>, grid, threads, smem, s, g.scratch, sample, g.H, g.W, probe, g.ph, pos, nframes,
                                                            rowgroups, grad_sample, grad_probe, g.row.tw, lines);
     } else if (const MixOps* mo = mix_ops(g.pw)) {
       MixRowsArgs a{sample, g.H, g.W, probe, g.ph, g.pw, pos, nframes, g.scratch, g.row.mix_twt, g.row.mix_twi,
@@ -915,10 +918,10 @@ void launch_cols(const BaseGeom& g, int frame0, int nframes, const uint16_t* mea
         // column DFT, amplitude-loss epilogue and inverse column DFT; counts fftshifted
         dim3 grid(num_tiles(g.pw), nframes);
         if (g.pw % kTile == 0) {
-          cols_sweep_pair<N, false, true, true, true><<<grid, ColPairCfg<N>::kThreads, ColPairCfg<N>::kSmemBytes, s>>>(
+          launch_pdl(cols_sweep_pair<N, false, true, true, true>, grid, ColPairCfg<N>::kThreads, ColPairCfg<N>::kSmemBytes, s,
               g.scratch, g.pw, frame0, g.col.tw, measured, g.lut, 1.0f, grad_scale, inv_numel, loss);
         } else {
-          cols_sweep_pair<N, false, true><<<grid, ColPairCfg<N>::kThreads, ColPairCfg<N>::kSmemBytes, s>>>(
+          launch_pdl(cols_sweep_pair<N, false, true>, grid, ColPairCfg<N>::kThreads, ColPairCfg<N>::kSmemBytes, s,
               g.scratch, g.pw, frame0, g.col.tw, measured, g.lut, 1.0f, grad_scale, inv_numel, loss);
         }
         return;
@@ -1070,7 +1073,7 @@ int ptx_base_sweep(const float* sample, int sample_h, int sample_w, const float*
   {
     const size_t ns = (size_t)sample_h * sample_w, np = (size_t)probe_h * probe_w;
     prof_begin(kMiscKernel, s);
-    sweep_prologue_kernel<<<prologue_blocks(ns, sm_count()), 256, 0, s>>>(GS, ns, GP, np, loss, g.err, g.lut, scale);
+    launch_pdl(sweep_prologue_kernel, prologue_blocks(ns, sm_count()), 256, 0, s, GS, ns, GP, np, loss, g.err, g.lut, scale);
     prof_end(kMiscKernel, s);
   }
   const float2* S = reinterpret_cast<const float2*>(sample);
@@ -1123,7 +1126,7 @@ int ptx_base_sweep_small(const float* sample, int sample_h, int sample_w, const 
   {
     const size_t ns = (size_t)sample_h * sample_w, np = (size_t)probe_h * probe_w;
     prof_begin(kMiscKernel, s);
-    sweep_prologue_kernel<<<prologue_blocks(ns, sm_count()), 256, 0, s>>>(GS, ns, GP, np, loss, g.err, g.lut, scale);
+    launch_pdl(sweep_prologue_kernel, prologue_blocks(ns, sm_count()), 256, 0, s, GS, ns, GP, np, loss, g.err, g.lut, scale);
     prof_end(kMiscKernel, s);
   }
   if (batch == 0) return cuda_status(cudaGetLastError(), "ptx_base_sweep_small launch");
@@ -1138,7 +1141,7 @@ int ptx_base_sweep_small(const float* sample, int sample_h, int sample_w, const 
       if (st) return;
       const int grid = persistent_grid((const void*)base_sweep_frame<N>, Cfg::kThreads, Cfg::kSmemBytes, batch);
       prof_begin(kBaseRowsForward, s);
-      base_sweep_frame<N><<<grid, Cfg::kThreads, Cfg::kSmemBytes, s>>>(S, sample_h, sample_w, P, positions_xy, batch,
+      launch_pdl(base_sweep_frame<N>, grid, Cfg::kThreads, Cfg::kSmemBytes, s, S, sample_h, sample_w, P, positions_xy, batch,
                                                                        measured, g.lut, grad_scale,
                                                                        1.0 / std::max(numel, 1.0), loss, GS, GP,
                                                                        g.row.tw, g.err);

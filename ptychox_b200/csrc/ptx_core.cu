@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <cstdarg>
@@ -164,12 +165,44 @@ int get_line_plan(int n, LinePlan* out) {
   return PTX_OK;
 }
 
+namespace {
+std::mutex g_smem_mutex;
+std::map<std::pair<int, const void*>, int> g_smem_cap;  // (device, kernel) -> cap already set
+}  // namespace
+
 int ensure_smem(const void* kernel, int bytes) {
   // the default 48 KB cap covers a kernel's static shared memory too (block reductions
   // keep up to a few hundred bytes there): raise the cap for anything within 1 KB of it
   if (bytes + 1024 <= 48 * 1024) return PTX_OK;
-  return cuda_status(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
-                     "cudaFuncSetAttribute(MaxDynamicSharedMemorySize)");
+  int dev = 0;
+  if (int st = cuda_status(cudaGetDevice(&dev), "cudaGetDevice")) return st;
+  const auto key = std::make_pair(dev, kernel);
+  {
+    std::lock_guard<std::mutex> lock(g_smem_mutex);
+    auto it = g_smem_cap.find(key);
+    if (it != g_smem_cap.end() && it->second >= bytes) return PTX_OK;
+  }
+  if (int st = cuda_status(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
+                           "cudaFuncSetAttribute(MaxDynamicSharedMemorySize)")) {
+    return st;
+  }
+  std::lock_guard<std::mutex> lock(g_smem_mutex);
+  int& cap = g_smem_cap[key];
+  cap = std::max(cap, bytes);
+  return PTX_OK;
+}
+
+void clear_smem_cache() {
+  std::lock_guard<std::mutex> lock(g_smem_mutex);
+  g_smem_cap.clear();
+}
+
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char* v = std::getenv("PTYCHOX_PDL");
+    return !(v && v[0] == '0');
+  }();
+  return on;
 }
 
 RowShape row_shape(const LinePlan& p, int rows_available) {
@@ -453,6 +486,7 @@ int ptx_clear_cache(void) {
   // place, so kernels still in flight never see another length's table.
   ptx::g_plans.clear();
   ptx::clear_noalloc_cache();
+  ptx::clear_smem_cache();
   return PTX_OK;
 }
 

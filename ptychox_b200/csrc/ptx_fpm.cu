@@ -54,6 +54,7 @@ __global__ void __launch_bounds__(128, 3) fpm_rows_forward(
     const float2* __restrict__ spec, int oh, int ow, const float2* __restrict__ pupil, int lh,
     const int64_t* __restrict__ led, int nframes, int rowgroups, float2* __restrict__ scratch,
     const float2* __restrict__ tw, int lines) {
+  pdl_wait();
   using S = RegShape<NW>;
   using Cfg = FpmRowCfg<NW>;
   constexpr int kTiles = (NW + kTile - 1) / kTile;
@@ -232,6 +233,7 @@ __global__ void __launch_bounds__(128, 3) fpm_rows_adjoint(
     const float2* __restrict__ pupil, int lh, const int64_t* __restrict__ led, int nframes, int rowgroups,
     float norm, float2* __restrict__ grad_spec, float2* __restrict__ grad_pupil, const float2* __restrict__ tw,
     int lines) {
+  pdl_wait();
   using S = RegShape<NW>;
   constexpr int kTiles = (NW + kTile - 1) / kTile;
   extern __shared__ float2 sm[];
@@ -446,7 +448,7 @@ void launch_fft2(const FpmGeom& g, const float2* in, int H, int W, float2* out, 
   dispatch_pow2(W, [&](auto NT) {
     constexpr int N = decltype(NT)::value;
     const int lines = RowPass<N>::lines(256, H);
-    fft2_rows_kernel<N, INV><<<(H + lines - 1) / lines, lines * RowPass<N>::T, RowPass<N>::smem(lines), s>>>(
+    launch_pdl(fft2_rows_kernel<N, INV>, (H + lines - 1) / lines, lines * RowPass<N>::T, RowPass<N>::smem(lines), s,
         in, H, tmp, prow.tw, lines);
   });
   prof_end(kFft2Rows, s);
@@ -454,7 +456,7 @@ void launch_fft2(const FpmGeom& g, const float2* in, int H, int W, float2* out, 
   dispatch_pow2(H, [&](auto NT) {
     constexpr int N = decltype(NT)::value;
     const int sm = kColsPerCta * ColPass<N>::LP * (int)sizeof(float2);
-    fft2_cols_kernel<N, INV><<<num_tiles(W) * (kTile / kColsPerCta), ColPass<N>::kThreads, sm, s>>>(
+    launch_pdl(fft2_cols_kernel<N, INV>, num_tiles(W) * (kTile / kColsPerCta), ColPass<N>::kThreads, sm, s,
         tmp, W, out, scale, pcol.tw);
   });
   prof_end(kFft2Cols, s);
@@ -476,7 +478,7 @@ void launch_rows_forward(const FpmGeom& g, const float2* spec, const float2* pup
     const int rowgroups = (g.lh + lines - 1) / lines;
     const int threads = lines * RowPass<N>::T, smem = FpmRowCfg<N>::smem(lines);
     const int grid = persistent_grid((const void*)fpm_rows_forward<N>, threads, smem, (long long)rowgroups * nf);
-    fpm_rows_forward<N><<<grid, threads, smem, s>>>(spec, g.oh, g.ow, pupil, g.lh, led, nf, rowgroups, g.frames,
+    launch_pdl(fpm_rows_forward<N>, grid, threads, smem, s, spec, g.oh, g.ow, pupil, g.lh, led, nf, rowgroups, g.frames,
                                                     g.p_lw.tw, lines);
   });
   prof_end(kFpmRowsForward, s);
@@ -501,10 +503,10 @@ void launch_cols(const FpmGeom& g, int frame0, int nf, const uint16_t* measured,
       // inverse column DFT, 1/(h w), amplitude-loss epilogue, forward column DFT
       dim3 grid(num_tiles(g.lw), nf);
       if (g.lw % kTile == 0) {
-        cols_sweep_pair<N, true, false, false, true><<<grid, ColPairCfg<N>::kThreads, ColPairCfg<N>::kSmemBytes, s>>>(
+        launch_pdl(cols_sweep_pair<N, true, false, false, true>, grid, ColPairCfg<N>::kThreads, ColPairCfg<N>::kSmemBytes, s,
             g.frames, g.lw, frame0, g.p_lh.tw, measured, g.lut, norm, grad_scale, inv_numel, loss);
       } else {
-        cols_sweep_pair<N, true, false><<<grid, ColPairCfg<N>::kThreads, ColPairCfg<N>::kSmemBytes, s>>>(
+        launch_pdl(cols_sweep_pair<N, true, false>, grid, ColPairCfg<N>::kThreads, ColPairCfg<N>::kSmemBytes, s,
             g.frames, g.lw, frame0, g.p_lh.tw, measured, g.lut, norm, grad_scale, inv_numel, loss);
       }
       return;
@@ -534,7 +536,7 @@ void launch_rows_adjoint(const FpmGeom& g, const float2* spec, const float2* pup
     const int rowgroups = (g.lh + lines - 1) / lines;
     const int threads = lines * RowPass<N>::T, smem = FpmRowCfg<N>::smem(lines);
     const int grid = persistent_grid((const void*)fpm_rows_adjoint<N>, threads, smem, (long long)rowgroups * nf);
-    fpm_rows_adjoint<N><<<grid, threads, smem, s>>>(g.frames, spec, g.oh, g.ow, pupil, g.lh, led, nf, rowgroups,
+    launch_pdl(fpm_rows_adjoint<N>, grid, threads, smem, s, g.frames, spec, g.oh, g.ow, pupil, g.lh, led, nf, rowgroups,
                                                     norm, grad_spec, grad_pupil, g.p_lw.tw, lines);
   });
   prof_end(kFpmRowsAdjoint, s);
@@ -623,7 +625,7 @@ int ptx_fpm_sweep(const float* object, int object_h, int object_w, const float* 
   {
     const size_t ns = g.spec_bytes / sizeof(float2), np = (size_t)low_h * low_w;
     prof_begin(kMiscKernel, s);
-    sweep_prologue_kernel<<<prologue_blocks(ns, sm_count()), 256, 0, s>>>(
+    launch_pdl(sweep_prologue_kernel, prologue_blocks(ns, sm_count()), 256, 0, s,
         g.gspec, ns, reinterpret_cast<float2*>(grad_pupil), np, loss, nullptr, g.lut, scale);
     prof_end(kMiscKernel, s);
   }

@@ -24,8 +24,36 @@ int get_line_plan(int n, LinePlan* out);
 bool size_supported(int n);
 
 // Raise a kernel's dynamic shared memory cap to `bytes` when they come near the 48 KB default
-// (which static shared memory also counts against).
+// (which static shared memory also counts against).  Remembered per (device, kernel), so
+// repeated calls cost no driver call; ptx_clear_cache forgets it.
 int ensure_smem(const void* kernel, int bytes);
+void clear_smem_cache();
+
+// Programmatic dependent launch: the sweep kernels are launched with programmatic stream
+// serialisation, so a grid is scheduled while the previous grid on the stream drains; each
+// such kernel starts with pdl_wait() (griddepcontrol.wait: it returns once the preceding
+// grid has completed and its writes are visible), so the order of memory effects is that of
+// plain stream order.  Off when the environment sets PTYCHOX_PDL=0 (read once).
+bool pdl_enabled();
+
+template <typename... KArgs, typename... Args>
+void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args&&... args) {
+  if (!pdl_enabled()) {
+    kernel<<<grid, block, smem, s>>>(static_cast<KArgs>(args)...);
+    return;
+  }
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
 
 inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 

@@ -90,6 +90,7 @@ struct ColCfg {
 // ---- rows forward: grid (frames, row groups of `lines` rows), lines * B threads -----------
 template <int N>
 __global__ void __launch_bounds__(RowCfg<N>::THREADS) mix_rows_forward(MixRowsArgs a, int lines) {
+  pdl_wait();
   using Cfg = RowCfg<N>;
   constexpr int A = Cfg::A, B = Cfg::B;
   extern __shared__ float2 sm[];
@@ -134,6 +135,7 @@ __global__ void __launch_bounds__(RowCfg<N>::THREADS) mix_rows_forward(MixRowsAr
 // probe through ld_nc_here, so neither is held in registers.
 template <int N>
 __global__ void __launch_bounds__(RowCfg<N>::THREADS, 2) mix_rows_adjoint(MixRowsArgs a, int lines, int fpc) {
+  pdl_wait();
   using Cfg = RowCfg<N>;
   constexpr int A = Cfg::A, B = Cfg::B;
   extern __shared__ float2 sm[];
@@ -205,6 +207,7 @@ __global__ void __launch_bounds__(RowCfg<N>::THREADS, 2) mix_rows_adjoint(MixRow
 // ---- columns: grid (tiles * 16 / C, frames) ---------------------------------------------
 template <int MODE, int N>
 __global__ void __launch_bounds__(ColCfg<N>::THREADS) mix_cols(MixColsArgs a) {
+  pdl_wait();
   using Cfg = ColCfg<N>;
   constexpr int A = Cfg::A, B = Cfg::B, C = Cfg::C;
   extern __shared__ float2 sm[];
@@ -352,7 +355,7 @@ struct Ops {
     if (a.nframes <= 0) return;
     const int lines = std::min(Cfg::LINES, a.ph);
     dim3 grid(a.nframes, (a.ph + lines - 1) / lines);
-    mix_rows_forward<N><<<grid, lines * Cfg::B, Cfg::smem_forward(lines), s>>>(a, lines);
+    launch_pdl(mix_rows_forward<N>, grid, lines * Cfg::B, Cfg::smem_forward(lines), s, a, lines);
   }
   static void rows_adjoint(const MixRowsArgs& a, cudaStream_t s) {
     using Cfg = RowCfg<N>;
@@ -364,18 +367,18 @@ struct Ops {
     int fpc = static_cast<int>(((long long)rowgroups * a.nframes) / std::max(target, 1LL));
     fpc = std::max(1, std::min(fpc, a.nframes));
     dim3 grid((a.nframes + fpc - 1) / fpc, rowgroups);
-    mix_rows_adjoint<N><<<grid, lines * Cfg::B, Cfg::smem_adjoint(lines), s>>>(a, lines, fpc);
+    launch_pdl(mix_rows_adjoint<N>, grid, lines * Cfg::B, Cfg::smem_adjoint(lines), s, a, lines, fpc);
   }
   static void cols(int mode, const MixColsArgs& a, cudaStream_t s) {
     using Cfg = ColCfg<N>;
     if (a.nframes <= 0) return;
     dim3 grid(num_tiles(a.pw) * (kTile / Cfg::C), a.nframes);
     if (mode == kMixColSweep) {
-      mix_cols<kMixColSweep, N><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(a);
+      launch_pdl(mix_cols<kMixColSweep, N>, grid, Cfg::THREADS, Cfg::SMEM, s, a);
     } else if (mode == kMixColForward) {
-      mix_cols<kMixColForward, N><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(a);
+      launch_pdl(mix_cols<kMixColForward, N>, grid, Cfg::THREADS, Cfg::SMEM, s, a);
     } else {
-      mix_cols<kMixColBackward, N><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(a);
+      launch_pdl(mix_cols<kMixColBackward, N>, grid, Cfg::THREADS, Cfg::SMEM, s, a);
     }
   }
   static const MixOps* table() {

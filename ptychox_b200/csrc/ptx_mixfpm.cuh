@@ -48,6 +48,7 @@ template <int N, bool PLUS>
 __global__ void __launch_bounds__(RowCfg<N>::THREADS) mix_fft2_rows(const float2* __restrict__ in, int H,
                                                                      float2* __restrict__ tiled,
                                                                      const float2* __restrict__ twt, int lines) {
+  pdl_wait();
   using Cfg = RowCfg<N>;
   constexpr int A = Cfg::A, B = Cfg::B;
   extern __shared__ float2 sm[];
@@ -78,6 +79,7 @@ template <int N, bool PLUS>
 __global__ void __launch_bounds__(ColCfg<N>::THREADS) mix_fft2_cols(const float2* __restrict__ tiled, int W,
                                                                      float2* __restrict__ out, float scale,
                                                                      const float2* __restrict__ twt) {
+  pdl_wait();
   using Cfg = ColCfg<N>;
   constexpr int A = Cfg::A, B = Cfg::B, C = Cfg::C;
   extern __shared__ float2 sm[];
@@ -106,6 +108,7 @@ __global__ void __launch_bounds__(ColCfg<N>::THREADS) mix_fft2_cols(const float2
 // ---- rows forward: grid (frames, row groups of `lines` rows) ------------------------------
 template <int N>
 __global__ void __launch_bounds__(RowCfg<N>::THREADS) mix_fpm_rows_forward(MixFpmRowsArgs a, int lines) {
+  pdl_wait();
   using Cfg = RowCfg<N>;
   constexpr int A = Cfg::A, B = Cfg::B;
   extern __shared__ float2 sm[];
@@ -154,6 +157,7 @@ __global__ void __launch_bounds__(RowCfg<N>::THREADS) mix_fpm_rows_forward(MixFp
 // registers across the CTA's frames.
 template <int N>
 __global__ void __launch_bounds__(RowCfg<N>::THREADS, 2) mix_fpm_rows_adjoint(MixFpmRowsArgs a, int lines, int fpc) {
+  pdl_wait();
   using Cfg = RowCfg<N>;
   constexpr int A = Cfg::A, B = Cfg::B;
   extern __shared__ float2 sm[];
@@ -230,6 +234,7 @@ __global__ void __launch_bounds__(RowCfg<N>::THREADS, 2) mix_fpm_rows_adjoint(Mi
 // ---- columns: grid (tiles * 16 / C, frames) ---------------------------------------------
 template <int MODE, int N>
 __global__ void __launch_bounds__(ColCfg<N>::THREADS) mix_fpm_cols(MixFpmColsArgs a) {
+  pdl_wait();
   using Cfg = ColCfg<N>;
   constexpr int A = Cfg::A, B = Cfg::B, C = Cfg::C;
   extern __shared__ float2 sm[];
@@ -368,9 +373,9 @@ struct Ops {
     const int lines = std::min(RC::LINES, H);
     const int grid = (H + lines - 1) / lines;
     if (plus) {
-      mix_fft2_rows<N, true><<<grid, lines * RC::B, RC::smem_forward(lines), s>>>(in, H, tiled, twt, lines);
+      launch_pdl(mix_fft2_rows<N, true>, grid, lines * RC::B, RC::smem_forward(lines), s, in, H, tiled, twt, lines);
     } else {
-      mix_fft2_rows<N, false><<<grid, lines * RC::B, RC::smem_forward(lines), s>>>(in, H, tiled, twt, lines);
+      launch_pdl(mix_fft2_rows<N, false>, grid, lines * RC::B, RC::smem_forward(lines), s, in, H, tiled, twt, lines);
     }
   }
   static void fft2_cols(bool plus, const float2* tiled, int W, float2* out, float scale, const float2* twt,
@@ -378,16 +383,16 @@ struct Ops {
     if (W <= 0) return;
     const int grid = num_tiles(W) * (kTile / CC::C);
     if (plus) {
-      mix_fft2_cols<N, true><<<grid, CC::THREADS, CC::SMEM, s>>>(tiled, W, out, scale, twt);
+      launch_pdl(mix_fft2_cols<N, true>, grid, CC::THREADS, CC::SMEM, s, tiled, W, out, scale, twt);
     } else {
-      mix_fft2_cols<N, false><<<grid, CC::THREADS, CC::SMEM, s>>>(tiled, W, out, scale, twt);
+      launch_pdl(mix_fft2_cols<N, false>, grid, CC::THREADS, CC::SMEM, s, tiled, W, out, scale, twt);
     }
   }
   static void rows_forward(const MixFpmRowsArgs& a, cudaStream_t s) {
     if (a.nframes <= 0) return;
     const int lines = std::min(RC::LINES, a.lh);
     dim3 grid(a.nframes, (a.lh + lines - 1) / lines);
-    mix_fpm_rows_forward<N><<<grid, lines * RC::B, RC::smem_forward(lines), s>>>(a, lines);
+    launch_pdl(mix_fpm_rows_forward<N>, grid, lines * RC::B, RC::smem_forward(lines), s, a, lines);
   }
   static void rows_adjoint(const MixFpmRowsArgs& a, cudaStream_t s) {
     if (a.nframes <= 0) return;
@@ -398,17 +403,17 @@ struct Ops {
     int fpc = static_cast<int>(((long long)rowgroups * a.nframes) / std::max(target, 1LL));
     fpc = std::max(1, std::min(fpc, a.nframes));
     dim3 grid((a.nframes + fpc - 1) / fpc, rowgroups);
-    mix_fpm_rows_adjoint<N><<<grid, lines * RC::B, RC::smem_adjoint(lines), s>>>(a, lines, fpc);
+    launch_pdl(mix_fpm_rows_adjoint<N>, grid, lines * RC::B, RC::smem_adjoint(lines), s, a, lines, fpc);
   }
   static void cols(int mode, const MixFpmColsArgs& a, cudaStream_t s) {
     if (a.nframes <= 0) return;
     dim3 grid(num_tiles(a.lw) * (kTile / CC::C), a.nframes);
     if (mode == kMixColSweep) {
-      mix_fpm_cols<kMixColSweep, N><<<grid, CC::THREADS, CC::SMEM, s>>>(a);
+      launch_pdl(mix_fpm_cols<kMixColSweep, N>, grid, CC::THREADS, CC::SMEM, s, a);
     } else if (mode == kMixColForward) {
-      mix_fpm_cols<kMixColForward, N><<<grid, CC::THREADS, CC::SMEM, s>>>(a);
+      launch_pdl(mix_fpm_cols<kMixColForward, N>, grid, CC::THREADS, CC::SMEM, s, a);
     } else {
-      mix_fpm_cols<kMixColBackward, N><<<grid, CC::THREADS, CC::SMEM, s>>>(a);
+      launch_pdl(mix_fpm_cols<kMixColBackward, N>, grid, CC::THREADS, CC::SMEM, s, a);
     }
   }
   static const MixFpmOps* table() {

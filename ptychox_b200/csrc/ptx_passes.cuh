@@ -90,6 +90,7 @@ static __global__ void decode_lut_kernel(float* __restrict__ lut, float scale) {
 static __global__ void sweep_prologue_kernel(float2* __restrict__ zero_a, size_t n_a, float2* __restrict__ zero_b,
                                              size_t n_b, double* __restrict__ loss, unsigned* __restrict__ err,
                                              float* __restrict__ lut, float scale) {
+  pdl_wait();
   const size_t stride = (size_t)gridDim.x * blockDim.x;
   const size_t i0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const float2 z = make_float2(0.f, 0.f);
@@ -163,6 +164,7 @@ template <int N, bool INV>
 __global__ void __launch_bounds__(256, 2) fft2_rows_kernel(const float2* __restrict__ in, int H,
                                                             float2* __restrict__ tiled,
                                                             const float2* __restrict__ tw, int lines) {
+  pdl_wait();
   using S = RegShape<N>;
   extern __shared__ float2 sm[];
   const int tid = threadIdx.x;
@@ -188,6 +190,7 @@ template <int N, bool INV>
 __global__ void __launch_bounds__(256, 2) fft2_cols_kernel(const float2* __restrict__ tiled, int W,
                                                             float2* __restrict__ out, float scale,
                                                             const float2* __restrict__ tw) {
+  pdl_wait();
   using S = RegShape<N>;
   extern __shared__ float2 sm[];
   const int tid = threadIdx.x;
@@ -244,6 +247,7 @@ __global__ void __launch_bounds__(ColPairCfg<N>::kThreads, col_pair_min_blocks<N
     float2* __restrict__ scratch, int width, int frame0, const float2* __restrict__ tw,
     const uint16_t* __restrict__ measured, const float* __restrict__ lut, float norm, float grad_scale,
     double inv_numel, double* __restrict__ loss) {
+  pdl_wait();
   using S = RegShape<N>;
   using Cfg = ColPairCfg<N>;
   extern __shared__ float4 sm4[];
