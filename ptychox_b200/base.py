@@ -198,7 +198,7 @@ def _prepare_subpixel(sample, probe, positions_xy):
 def _subpixel_ws_bytes(ph, pw, batch):
     n = _abi.query("ptx_base_subpix_workspace_bytes", ph, pw, batch)
     if n == 0:
-        raise ValueError(f"sub-pixel scans take probe sides that are powers of two in [16, 1024] (got {ph}x{pw}).")
+        raise ValueError(f"sub-pixel scans take probe sides that are 2^a 3^b 5^c in [16, 1024] (got {ph}x{pw}).")
     return n
 
 
@@ -288,7 +288,7 @@ def ptychoX_base_subpixel(sample: torch.Tensor, probe: torch.Tensor, positions_x
     Each frame crops the window at ``floor(p + 1/2)`` and shifts it by the fractional part
     with a Fourier phase ramp (the reference's ``shift_phase_ramp``, ``coded/ops.py:157-171``,
     applied to the patch), so ``(x, y)`` samples the object at ``(x + c, y + r)``.  At
-    integer positions this is :func:`ptychoX_base`.  Probe sides: powers of two in [16, 1024].
+    integer positions this is :func:`ptychoX_base`.  Probe sides: 2^a 3^b 5^c in [16, 1024].
     Differentiable in ``sample`` and ``probe``.
     """
     return PtychoXBaseSubpixelFunction.apply(sample, probe, positions_xy)

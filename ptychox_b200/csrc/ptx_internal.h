@@ -279,4 +279,38 @@ struct MixCodedOps {
 };
 const MixCodedOps* mix_coded_ops(int n);
 
+// ---- sub-pixel conventional passes on the mixed-radix engine (ptx_mixsubpix.cuh) ---------
+// Probe sides that are {2,3,5}-smooth but not powers of two, 16..1000 (mix_subpix_ops(n) is
+// null for every other side); the column passes run on the column side ph, the row passes on
+// the row side pw.
+struct MixSubpixArgs {
+  const float2* sample;  // object, H x W (gather)
+  float2* grad_sample;   // scatter target
+  int H, W, ph, pw;
+  const double* pos;     // float (x, y) of every frame of the batch
+  int frame0, nframes;   // this chunk
+  float2* scratch;       // tiled frames [frame][tile][row][16] of the chunk
+  float2* sbuf;          // the shifted patches S, same layout
+  const float2* rx;      // row ramps [batch][pw], column ramps [batch][ph] (1/n folded in)
+  const float2* ry;
+  const float2* probe;
+  float2* grad_probe;
+  const float2* twt_col;  // mixed-radix twiddles of ph and pw
+  const float2* twi_col;
+  const float2* twt_row;
+  const float2* twi_row;
+};
+enum MixSubpixRows {
+  kMixSubpixSweepForward = 0,  // shift (S stored), x P, row DFT (stored)
+  kMixSubpixShiftOnly = 1,     // shift (S stored)
+  kMixSubpixForwardOnly = 2,   // shift, x P, row DFT (stored)
+  kMixSubpixAdjoint = 3        // inverse row DFT, grad_P, x conj(P), row DFT, opposite shift
+};
+struct MixSubpixOps {
+  int (*prepare)();
+  void (*cols)(bool gather, const MixSubpixArgs&, cudaStream_t);  // column side ph
+  void (*rows)(int variant, const MixSubpixArgs&, cudaStream_t);  // row side pw
+};
+const MixSubpixOps* mix_subpix_ops(int n);
+
 }  // namespace ptx

@@ -18,8 +18,9 @@
 //   5. columns: the column shift's adjoint (column DFT, x conj(ramp_y), inverse) and the
 //               scatter-add into grad_O at the window.
 // The ramps (with the inverse transforms' 1/n folded in) are tabulated per frame in FP64 by a
-// prologue kernel and rounded once to FP32.  Frame sides are powers of two in [16, 1024] (the
-// register FFT).
+// prologue kernel and rounded once to FP32.  Frame sides are {2,3,5}-smooth in [16, 1024]:
+// powers of two run the register-FFT kernels below, other sides the mixed-radix kernels of
+// ptx_mixsubpix.cuh (each pass picks by the side it transforms), through the same layout.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -61,7 +62,7 @@ __global__ void subpix_ramp_kernel(const double* __restrict__ pos, int nframes, 
     const int kk = along_x ? k : k - pw;
     const double p = pos[2 * f + (along_x ? 0 : 1)];
     const double d = p - floor(p + 0.5);
-    const int kf = kk < n / 2 ? kk : kk - n;
+    const int kf = kk <= (n - 1) / 2 ? kk : kk - n;  // numpy fftfreq * n, odd n too
     double s, c;
     sincospi(2.0 * d * kf / n, &s, &c);
     const float2 v = make_float2(static_cast<float>(c / n), static_cast<float>(s / n));
@@ -99,9 +100,10 @@ __global__ void __launch_bounds__(kSpCols * RegShape<N>::T) subpix_cols_kernel(
   const int ct = blockIdx.x / kSubs;
   const int c0 = ct * kTile + (blockIdx.x - ct * kSubs) * kSpCols;
   const int kc = c0 + c;
+  const bool col_ok = kc < pw;
   const int f = blockIdx.y;
   const int g = frame0 + f;
-  const int tiles = pw / kTile;
+  const int tiles = num_tiles(pw);
   float2* tile = scratch + ((size_t)f * tiles + ct) * N * kTile + (c0 - ct * kTile);
   long long x0, y0;
   sp_corner(pos, g, x0, y0);
@@ -112,10 +114,10 @@ __global__ void __launch_bounds__(kSpCols * RegShape<N>::T) subpix_cols_kernel(
   if (GATHER) {
     const float2* col = sample + y0 * W + x0 + kc;
 #pragma unroll
-    for (int j = 0; j < S::N1; ++j) v[j] = ok ? __ldg(&col[(size_t)(t + S::T * j) * W]) : make_float2(0.f, 0.f);
+    for (int j = 0; j < S::N1; ++j) v[j] = (ok && col_ok) ? __ldg(&col[(size_t)(t + S::T * j) * W]) : make_float2(0.f, 0.f);
   } else {
 #pragma unroll
-    for (int j = 0; j < S::N1; ++j) v[j] = tile[(t + S::T * j) * kTile + c];
+    for (int j = 0; j < S::N1; ++j) v[j] = col_ok ? tile[(t + S::T * j) * kTile + c] : make_float2(0.f, 0.f);
   }
   reg_fft<N, false, true>(v, buf, t, tw);
 #pragma unroll
@@ -126,9 +128,11 @@ __global__ void __launch_bounds__(kSpCols * RegShape<N>::T) subpix_cols_kernel(
   }
   reg_fft<N, true, true>(v, buf, t, tw);
   if (GATHER) {
+    if (col_ok) {
 #pragma unroll
-    for (int j = 0; j < S::N1; ++j) tile[(t + S::T * j) * kTile + c] = v[j];
-  } else if (ok) {
+      for (int j = 0; j < S::N1; ++j) tile[(t + S::T * j) * kTile + c] = v[j];
+    }
+  } else if (ok && col_ok) {
     float2* col = grad_sample + y0 * W + x0 + kc;
 #pragma unroll
     for (int j = 0; j < S::N1; ++j) atomicAdd(&col[(size_t)(t + S::T * j) * W], v[j]);
@@ -225,9 +229,10 @@ __global__ void __launch_bounds__(kSpRowThreads) subpix_rows_kernel(
   }
 }
 
-bool sp_side_ok(int n) { return n >= 16 && n <= 1024 && (n & (n - 1)) == 0; }
+bool sp_side_ok(int n) { return n >= 16 && n <= 1024 && ((n & (n - 1)) == 0 || mix_subpix_ops(n) != nullptr); }
 
-size_t sp_frame_bytes(int ph, int pw) { return (size_t)ph * pw * sizeof(float2); }
+// a tiled frame [tile][row][16]
+size_t sp_frame_bytes(int ph, int pw) { return (size_t)num_tiles(pw) * kTile * ph * sizeof(float2); }
 
 size_t sp_ramp_bytes(int ph, int pw, int batch) {
   return align_up((size_t)std::max(batch, 1) * (ph + pw) * sizeof(float2), 256);
@@ -236,6 +241,8 @@ size_t sp_ramp_bytes(int ph, int pw, int batch) {
 struct SpGeom {
   int H, W, ph, pw, batch, chunk;
   LinePlan row, col;
+  const MixSubpixOps* mcol;  // mixed-radix column passes (ph not a power of two), else null
+  const MixSubpixOps* mrow;  // mixed-radix row passes (pw not a power of two), else null
   unsigned* err;
   float* lut;
   float2* rx;
@@ -250,7 +257,7 @@ int sp_check(const void* sample, int H, int W, const void* probe, int ph, int pw
   if (H <= 0 || W <= 0 || batch < 0) return set_error(PTX_ERR_INVALID_ARGUMENT, "non-positive shape");
   if (!sp_side_ok(ph) || !sp_side_ok(pw)) {
     return set_error(PTX_ERR_UNSUPPORTED_SIZE,
-                     "sub-pixel sweeps take probe sides that are powers of two in [16, 1024] (got %d x %d)", ph, pw);
+                     "sub-pixel sweeps take probe sides that are 2^a 3^b 5^c in [16, 1024] (got %d x %d)", ph, pw);
   }
   if (ph > H || pw > W) {
     return set_error(PTX_ERR_INVALID_ARGUMENT, "probe (%d x %d) larger than sample (%d x %d)", ph, pw, H, W);
@@ -265,16 +272,32 @@ int sp_check(const void* sample, int H, int W, const void* probe, int ph, int pw
                      ws_bytes, fixed + 2 * frame);
   }
   g->H = H; g->W = W; g->ph = ph; g->pw = pw; g->batch = batch;
-  g->chunk = static_cast<int>(std::min<size_t>((ws_bytes - fixed) / (2 * frame), (size_t)std::max(batch, 1)));
+  // frames per chunk: what the workspace holds, at most the batch and 65535 (a grid dimension)
+  g->chunk = static_cast<int>(
+      std::min<size_t>({(ws_bytes - fixed) / (2 * frame), (size_t)std::max(batch, 1), (size_t)65535}));
   if (int st = get_line_plan(pw, &g->row)) return st;
   if (int st = get_line_plan(ph, &g->col)) return st;
+  g->mcol = (ph & (ph - 1)) ? mix_subpix_ops(ph) : nullptr;
+  g->mrow = (pw & (pw - 1)) ? mix_subpix_ops(pw) : nullptr;
+  if ((g->mcol && !g->col.mix_twt) || (g->mrow && !g->row.mix_twt)) {
+    return set_error(PTX_ERR_UNSUPPORTED_SIZE, "no mixed-radix twiddle tables for %d x %d", ph, pw);
+  }
+  if (g->mcol) {
+    if (int st = g->mcol->prepare()) return st;
+  }
+  if (g->mrow) {
+    if (int st = g->mrow->prepare()) return st;
+  }
+  if (const MixOps* mo = (ph & (ph - 1)) ? mix_ops(ph) : nullptr) {  // the loss column pass
+    if (int st = mo->prepare()) return st;
+  }
   char* base = static_cast<char*>(ws);
   g->err = reinterpret_cast<unsigned*>(base);
   g->lut = reinterpret_cast<float*>(base + 256);
   g->rx = reinterpret_cast<float2*>(base + kSpHeader);
   g->ry = g->rx + (size_t)std::max(batch, 1) * pw;
   g->scratch = reinterpret_cast<float2*>(base + fixed);
-  g->sbuf = g->scratch + (size_t)g->chunk * ph * pw;
+  g->sbuf = g->scratch + (size_t)g->chunk * (frame / sizeof(float2));  // tiled frames, padded tiles included
   return PTX_OK;
 }
 
@@ -287,9 +310,38 @@ void sp_launch_ramps(const SpGeom& g, const double* pos, cudaStream_t s) {
   prof_end(kMiscKernel, s);
 }
 
+MixSubpixArgs sp_mix_args(const SpGeom& g, const double* pos, int frame0, int nf) {
+  MixSubpixArgs a{};
+  a.H = g.H;
+  a.W = g.W;
+  a.ph = g.ph;
+  a.pw = g.pw;
+  a.pos = pos;
+  a.frame0 = frame0;
+  a.nframes = nf;
+  a.scratch = g.scratch;
+  a.sbuf = g.sbuf;
+  a.rx = g.rx;
+  a.ry = g.ry;
+  a.twt_col = g.col.mix_twt;
+  a.twi_col = g.col.mix_twi;
+  a.twt_row = g.row.mix_twt;
+  a.twi_row = g.row.mix_twi;
+  return a;
+}
+
 template <bool GATHER>
 int sp_launch_cols(const SpGeom& g, const float2* sample, float2* grad_sample, const double* pos, int frame0, int nf,
                    cudaStream_t s) {
+  if (g.mcol) {
+    MixSubpixArgs a = sp_mix_args(g, pos, frame0, nf);
+    a.sample = sample;
+    a.grad_sample = grad_sample;
+    prof_begin(kSubpixCols, s);
+    g.mcol->cols(GATHER, a, s);
+    prof_end(kSubpixCols, s);
+    return PTX_OK;
+  }
   int st = PTX_OK;
   dispatch_pow2(g.ph, [&](auto NT) {
     constexpr int N = decltype(NT)::value;
@@ -298,7 +350,7 @@ int sp_launch_cols(const SpGeom& g, const float2* sample, float2* grad_sample, c
       const int smem = kSpCols * col_line_pitch<N>() * (int)sizeof(float2);
       st = ensure_smem((const void*)subpix_cols_kernel<N, GATHER>, smem);
       if (st) return;
-      dim3 grid((g.pw / kTile) * (kTile / kSpCols), nf);
+      dim3 grid(num_tiles(g.pw) * (kTile / kSpCols), nf);
       prof_begin(kSubpixCols, s);
       subpix_cols_kernel<N, GATHER><<<grid, threads, smem, s>>>(sample, grad_sample, g.H, g.W, g.pw, pos, frame0,
                                                                 g.scratch, g.ry, g.col.tw);
@@ -309,7 +361,20 @@ int sp_launch_cols(const SpGeom& g, const float2* sample, float2* grad_sample, c
 }
 
 template <bool FORWARD, bool STORE_S, bool STORE_OUT>
-int sp_launch_rows(const SpGeom& g, const float2* probe, float2* grad_probe, int frame0, int nf, cudaStream_t s) {
+int sp_launch_rows(const SpGeom& g, const float2* probe, float2* grad_probe, int frame0, int nf, cudaStream_t s,
+                   const double* pos) {
+  if (g.mrow) {
+    MixSubpixArgs a = sp_mix_args(g, pos, frame0, nf);
+    a.probe = probe;
+    a.grad_probe = grad_probe;
+    const int variant = !FORWARD ? kMixSubpixAdjoint
+                        : (STORE_S && STORE_OUT) ? kMixSubpixSweepForward
+                        : STORE_S ? kMixSubpixShiftOnly : kMixSubpixForwardOnly;
+    prof_begin(kSubpixRows, s);
+    g.mrow->rows(variant, a, s);
+    prof_end(kSubpixRows, s);
+    return PTX_OK;
+  }
   int st = PTX_OK;
   dispatch_pow2(g.pw, [&](auto NT) {
     constexpr int M = decltype(NT)::value;
@@ -336,14 +401,23 @@ int sp_launch_rows(const SpGeom& g, const float2* probe, float2* grad_probe, int
 
 int sp_launch_cols_sweep(const SpGeom& g, int frame0, int nf, const uint16_t* measured, float grad_scale,
                          double inv_numel, double* loss, cudaStream_t s) {
+  if (const MixOps* mo = (g.ph & (g.ph - 1)) ? mix_ops(g.ph) : nullptr) {
+    MixColsArgs a{g.scratch, g.ph, g.pw, frame0, nf, g.col.mix_twt, g.col.mix_twi, measured, g.lut,
+                  grad_scale, inv_numel, loss, nullptr, nullptr, nullptr};
+    prof_begin(kBaseCols, s);
+    mo->cols(kMixColSweep, a, s);
+    prof_end(kBaseCols, s);
+    return PTX_OK;
+  }
   int st = PTX_OK;
   dispatch_pow2(g.ph, [&](auto NT) {
     constexpr int N = decltype(NT)::value;
     if constexpr (N >= 16) {
-      auto kern = cols_sweep_pair<N, false, true, true, true>;
+      // the full-tile variant needs whole 16-column tiles
+      auto kern = (g.pw % kTile == 0) ? cols_sweep_pair<N, false, true, true, true> : cols_sweep_pair<N, false, true, true>;
       st = ensure_smem((const void*)kern, ColPairCfg<N>::kSmemBytes);
       if (st) return;
-      dim3 grid(g.pw / kTile, nf);
+      dim3 grid(num_tiles(g.pw), nf);
       prof_begin(kBaseCols, s);
       kern<<<grid, ColPairCfg<N>::kThreads, ColPairCfg<N>::kSmemBytes, s>>>(g.scratch, g.pw, frame0, g.col.tw,
                                                                             measured, g.lut, 1.0f, grad_scale,
@@ -399,9 +473,9 @@ int ptx_base_subpix_sweep(const float* sample, int sample_h, int sample_w, const
   for (int b0 = 0; b0 < batch; b0 += g.chunk) {
     const int nf = std::min(g.chunk, batch - b0);
     int st = sp_launch_cols<true>(g, S, nullptr, positions_xy, b0, nf, s);
-    if (!st) st = sp_launch_rows<true, true, true>(g, P, nullptr, b0, nf, s);
+    if (!st) st = sp_launch_rows<true, true, true>(g, P, nullptr, b0, nf, s, positions_xy);
     if (!st) st = sp_launch_cols_sweep(g, b0, nf, measured, grad_scale, 1.0 / std::max(numel, 1.0), loss, s);
-    if (!st) st = sp_launch_rows<false, false, false>(g, P, GP, b0, nf, s);
+    if (!st) st = sp_launch_rows<false, false, false>(g, P, GP, b0, nf, s, positions_xy);
     if (!st) st = sp_launch_cols<false>(g, nullptr, GS, positions_xy, b0, nf, s);
     if (st) return st;
   }
@@ -425,7 +499,7 @@ int ptx_base_subpix_forward(const float* sample, int sample_h, int sample_w, con
   for (int b0 = 0; b0 < batch; b0 += g.chunk) {
     const int nf = std::min(g.chunk, batch - b0);
     int st = sp_launch_cols<true>(g, S, nullptr, positions_xy, b0, nf, s);
-    if (!st) st = sp_launch_rows<true, false, true>(g, P, nullptr, b0, nf, s);
+    if (!st) st = sp_launch_rows<true, false, true>(g, P, nullptr, b0, nf, s, positions_xy);
     if (!st) {
       st = base_cols_pass(true, g.scratch, probe_h, probe_w, b0, nf, reinterpret_cast<float2*>(far_field), amplitude,
                           nullptr, s);
@@ -460,12 +534,12 @@ int ptx_base_subpix_backward(const float* grad_output, const float* far_field, c
     const int nf = std::min(g.chunk, batch - b0);
     // the shifted patches S (for the probe gradient), then g F/|F| through the inverse column DFT
     int st = sp_launch_cols<true>(g, S, nullptr, positions_xy, b0, nf, s);
-    if (!st) st = sp_launch_rows<true, true, false>(g, P, nullptr, b0, nf, s);
+    if (!st) st = sp_launch_rows<true, true, false>(g, P, nullptr, b0, nf, s, positions_xy);
     if (!st) {
       st = base_cols_pass(false, g.scratch, probe_h, probe_w, b0, nf,
                           const_cast<float2*>(reinterpret_cast<const float2*>(far_field)), nullptr, grad_output, s);
     }
-    if (!st) st = sp_launch_rows<false, false, false>(g, P, GP, b0, nf, s);
+    if (!st) st = sp_launch_rows<false, false, false>(g, P, GP, b0, nf, s, positions_xy);
     if (!st) st = sp_launch_cols<false>(g, nullptr, GS, positions_xy, b0, nf, s);
     if (st) return st;
   }
