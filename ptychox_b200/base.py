@@ -113,6 +113,15 @@ class PtychoXBaseFunction(torch.autograd.Function):
 
 
 SMALL_FRAMES = (32, 64, 128)
+# 128^2 frames take the one-CTA-per-frame sweep only from this many frames up: that kernel
+# costs about one CTA's latency per wave of frames (~30 us on a B200), the three passes
+# ~11 us + 0.21 us per frame (36 frames: 18.5 against 30.5 us; 121: 36.3 against 31.9 us)
+SMALL_128_MIN_FRAMES = 96
+
+
+def use_small_sweep(ph: int, pw: int, batch: int) -> bool:
+    """Whether a conventional sweep runs ``ptx_base_sweep_small`` (one CTA per frame)."""
+    return ph == pw and pw in SMALL_FRAMES and (pw < 128 or batch >= SMALL_128_MIN_FRAMES)
 
 
 def base_sweep(sample, probe, positions, measured, scale, ws=None):
@@ -130,7 +139,7 @@ def base_sweep(sample, probe, positions, measured, scale, ws=None):
     if ws is None:
         ws = workspace(_abi.query("ptx_base_workspace_bytes", ph, pw, batch), dev)
     # square 32 / 64 / 128 probes: the one-CTA-per-frame sweep (frame resident in shared memory)
-    entry = "ptx_base_sweep_small" if ph == pw and pw in SMALL_FRAMES else "ptx_base_sweep"
+    entry = "ptx_base_sweep_small" if use_small_sweep(ph, pw, batch) else "ptx_base_sweep"
     with torch.cuda.device(dev):
         _abi.call(entry, ptr(sample), sample.shape[0], sample.shape[1], ptr(probe), ph, pw,
                   ptr(positions), batch, ptr(measured), float(scale), ptr(loss), ptr(gs), ptr(gp), ptr(ws),

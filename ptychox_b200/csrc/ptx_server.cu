@@ -145,7 +145,11 @@ size_t slot_bytes(const Request& r) {
 int run_sweep(const Slot& s) {
   const ptx_recon_request& d = s.req->d;
   if (d.modality == PTX_MODALITY_CONVENTIONAL) {
-    const bool small = d.aux_h == d.aux_w && (d.aux_w == 32 || d.aux_w == 64 || d.aux_w == 128);
+    // one CTA per frame for square 32 / 64 / 128 probes; for 128^2 frames only from 96 frames
+    // up (one such CTA takes ~30 us per wave of frames, the three passes ~11 us + 0.21 us per
+    // frame on a B200)
+    const bool small = d.aux_h == d.aux_w &&
+                       (d.aux_w == 32 || d.aux_w == 64 || (d.aux_w == 128 && d.batch >= 96));
     return (small ? ptx_base_sweep_small : ptx_base_sweep)(
         s.obj, d.obj_h, d.obj_w, s.aux, d.aux_h, d.aux_w, static_cast<const int64_t*>(s.scan), d.batch, s.meas,
         d.scale, s.loss, s.g_obj, s.g_aux, s.ws, s.req->ws_bytes, s.stream);

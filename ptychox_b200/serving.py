@@ -33,6 +33,7 @@ import torch.nn.functional as F
 
 from . import _abi
 from ._utils import ptr
+from .base import use_small_sweep
 from .optim import FusedAdam
 
 __all__ = ["ReconRequest", "ReconResult", "ReconstructionServer", "run_plain", "percentile"]
@@ -172,7 +173,7 @@ class _Slot:
         s = self.stream_handle
         if r.modality == "conventional":
             (h, w), (ph, pw) = self.obj.shape, self.aux.shape
-            entry = "ptx_base_sweep_small" if ph == pw and pw in (32, 64, 128) else "ptx_base_sweep"
+            entry = "ptx_base_sweep_small" if use_small_sweep(ph, pw, r.units()) else "ptx_base_sweep"
             _abi.call(entry, ptr(self.obj), h, w, ptr(self.aux), ph, pw, ptr(self.pos), r.units(),
                       ptr(self.meas), float(r.scale), ptr(self.loss), ptr(self.g_obj), ptr(self.g_aux), ptr(self.ws),
                       self.ws.numel(), s)
