@@ -445,7 +445,8 @@ class ClockSampler:
 MEASURED_TRAFFIC = {
     "conventional-900x512-2048": (7.319e9, "profiles/base_sweep_kernels_96positions_full.md",
                                   "96-position capture scaled by 900/96"),
-    "fourier-225x256-1024": (0.4376e9, "profiles/fpm_sweep_225x256_full.md", "full-size capture"),
+    "fourier-225x256-1024": (0.4366e9, "profiles/fpm_sweep_225x256_full.md",
+                             "full-size captures, one per kernel"),
     "coded-64x1024-ds4": (6.60e9, "profiles/coded_sweep_16x1024_full.md", "16-shift capture scaled by 64/16"),
 }
 
