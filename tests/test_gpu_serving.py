@@ -42,7 +42,14 @@ def test_alone_equals_mixed_and_plain():
         assert rel_l2(res.aux, alone.aux) < 1e-4
     plain = run_plain(reqs, "cuda", realtime=False)
     for res, pl in zip(mixed, plain):
-        # same math through the unfused operators and torch.optim.Adam
+        # same math through the unfused operators and torch.optim.Adam.  The bar is 1e-3, not
+        # 1e-5: with eps 1e-16 an Adam step is close to lr * sign(g) per real component, so a
+        # gradient component at FP32 rounding level can take opposite signs in the fused sweep
+        # and in the unfused operators and move that pixel by 2 lr, and 12 iterations carry
+        # such moves forward.  The parts are held tightly on their own: the fused sweeps and
+        # the operators to 1e-5 against the FP64 oracle (test_gpu_base, test_gpu_fpm,
+        # test_gpu_coded) and the fused Adam step to 1e-6 against torch.optim.Adam
+        # (test_gpu_adam).
         assert abs(res.final_loss - pl.final_loss) <= 1e-3 * abs(pl.final_loss)
         assert rel_l2(res.obj, pl.obj) < 1e-3
 
