@@ -75,7 +75,7 @@ def small_problem(n_obj, p, grid, step, origin, jitter, photons, seed):
 
 @pytest.mark.parametrize("p", [32, 64, 96, 128, 160])
 def test_sweep_vs_oracle_sizes(p):
-    """Compile-time (32, 64, 128) and runtime-plan (96, 160) transform lengths."""
+    """Power-of-two (32, 64, 128) and mixed-radix (96 = 8 x 12, 160 = 10 x 16) transform lengths."""
     obj, probe, pos, meas, scale = small_problem(4 * p, p, 4, p // 2, 3, 2, 1e4, seed=p)
     loss, gs, gp = run_sweep(obj, probe, pos, meas, scale)
     rl, rs, rp = O.base_sweep(obj, probe, pos, meas, scale)

@@ -21,7 +21,7 @@ def small_mix():
         (0, "conventional", {"p": 64, "grid": 5, "step": 16, "n": 160}),
         (1, "fourier", {"n": 128, "h": 32, "grid": 5}),
         (2, "coded", {"n": 64, "count": 6, "ds": 2}),
-        (3, "conventional", {"p": 96, "grid": 4, "step": 24, "n": 208}),  # runtime-plan length
+        (3, "conventional", {"p": 96, "grid": 4, "step": 24, "n": 208}),  # mixed-radix length
         (4, "nearfield", {"n": 64, "count": 5, "ds": 4}),
         (5, "fourier", {"n": 64, "h": 16, "grid": 3}),
     ]
