@@ -7,6 +7,9 @@
 // DFT in registers, synchronises, and writes the outputs back in Stockham autosort
 // order, so the result is in natural order with no bit reversal.  Radices 2, 3, 4, 5,
 // 8 and 16 are supported; the plan (radix sequence) is chosen on the host.
+// The register engines (ptx_regfft.cuh / ptx_pairfft.cuh for powers of two from 16,
+// ptx_mixfft.cuh for the other smooth lengths from 6) take every longer line, so in the
+// sweeps this engine serves only lengths 2 .. 8 (ptx_fft_engine in include/ptychox.h).
 //
 // Twiddles come from a per-size table exp(-2 pi i m / n), m < n, computed on the host in
 // FP64 (std::cos / std::sin) and rounded once to FP32.  Both directions are
